@@ -1,0 +1,62 @@
+"""Build recipe for the star-join engine: nvcc -> in-tree shared library.
+
+The CUDA sources under csrc/ compile for sm_100a only into
+_build/libstarjoin.so (in-tree, so it travels with the repository snapshot).
+A rebuild happens when any source or header is newer than the library.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(BUILD, "libstarjoin.so")
+
+SOURCES = ["sj_engine.cu", "sj_build.cu", "sj_probe.cu", "sj_batch.cu"]
+HEADERS = ["sj_internal.h", "sj_ptx.cuh", "sj_datagen.h"]
+GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+              "-Xcompiler", "-pthread"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def _sources() -> list[str]:
+    return [os.path.join(CSRC, s) for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build_engine(force: bool = False, verbose: bool = False) -> str:
+    """Compile csrc/*.cu into _build/libstarjoin.so; return its path."""
+    srcs = _sources()
+    deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [
+        os.path.join(ROOT, "include", "starjoin.h")]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    os.makedirs(BUILD, exist_ok=True)
+    tmp = LIB + ".tmp"
+    cmd = [_nvcc(), *GENCODE, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-o", tmp, *srcs]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build_engine(force="--force" in sys.argv, verbose=True))

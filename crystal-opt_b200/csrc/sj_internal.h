@@ -1,0 +1,152 @@
+// sj_internal.h -- device-side data structures shared by the build, probe and
+// finalize kernels and the host orchestration (not part of the C ABI).
+#pragma once
+#include <cstdint>
+
+#include "../../include/starjoin.h"
+
+namespace sj {
+
+constexpr int kMaxDims = SJ_MAX_DIMS;
+constexpr int kMaxSteps = 2 * SJ_MAX_DIMS;
+constexpr uint32_t kMaxPolls = 1u << 22;  // bounded mbarrier waits (~0.5 s with backoff)
+
+// Device error bits (SjDesc::error_flags).
+enum : uint32_t {
+  kErrPayloadDomain = 1u << 0,  // a grouped payload fell outside [payload_min, payload_max]
+  kErrWaitTimeout = 1u << 1,    // a bounded mbarrier wait expired
+  kErrQueueOverflow = 1u << 2,  // internal survivor queue overflow (must never happen)
+};
+
+// Filter layouts.
+enum : uint32_t {
+  kBfDirect = 0,   // one bit per PHT slot, 32-bit words (crystal/bloom.cuh layout)
+  kBfBlocked = 1,  // k bits inside one 64-bit word per key (register-blocked)
+};
+
+// Per-dimension state the build kernels compute on the device.
+struct SjDimDev {
+  uint32_t n_inserted;     // qualifying dimension rows
+  uint32_t bf_log2;        // blocked: log2(#64-bit words); direct: log2(#bits)
+  uint32_t n_codes;        // distinct payload values of qualifying rows (grouped dims)
+  uint32_t group_stride;   // multiplier of the dim's code in the group index
+};
+
+// Per-query device descriptor (build writes, probe/finalize read, host fetches).
+struct SjDesc {
+  SjDimDev dim[kMaxDims];
+  uint32_t n_groups;
+  uint32_t error_flags;
+  uint32_t groups_out;     // finalize: number of rows written
+  uint32_t pad0;
+  unsigned long long rows_scanned;
+  unsigned long long step_in[kMaxSteps];
+  unsigned long long step_out[kMaxSteps];
+  unsigned long long bf_probes[kMaxDims];
+  unsigned long long bf_passes[kMaxDims];
+  unsigned long long reorders;
+};
+
+// Runtime parameters of one dimension in the kernels.
+struct SjDimRt {
+  const int32_t* fact_fk;
+  const int32_t* key;
+  const int32_t* filter_attr;
+  const int32_t* payload;
+  const uint32_t* in_bitmap;  // SJ_PRED_IN: bitmap over [0, SJ_MAX_IN_CODES)
+  int2* ht;                   // [key, value] slots
+  void* bf;                   // filter words
+  uint32_t* payload_bitmap;   // grouped: bitmap over the payload domain
+  int32_t* dict;              // grouped: code -> payload
+  uint64_t rows;
+  uint64_t fastmod_m;         // ceil(2^64 / ht_len) for the slot reduction
+  int32_t key_min;
+  uint32_t ht_len;
+  int32_t pred_kind, pred_lo, pred_hi;
+  int32_t payload_min;
+  uint32_t payload_span;
+  uint32_t grouped;
+  uint32_t bf_mode;
+  uint32_t bf_k;
+  uint32_t bf_bits_per_key;
+  uint32_t bf_max_log2;       // capacity of the allocated filter
+};
+
+struct SjPlanRt {
+  SjDimRt dim[kMaxDims];
+  SjDesc* desc;
+  const int32_t* measure;
+  const int32_t* measure_sub;
+  unsigned long long* g_sum;
+  unsigned long long* g_cnt;
+  sj_group_row* rows_out;
+  uint64_t row_begin, row_end;
+  uint32_t n_dims;
+  uint32_t lip;
+  uint32_t adaptive;
+  uint32_t order[kMaxDims];
+  uint32_t group_capacity;    // allocated dense group slots
+};
+
+// Launch geometry of the probe kernel.
+struct SjProbeGeom {
+  uint32_t threads;
+  uint32_t chunk_rows;
+  uint32_t stages;
+  uint32_t grid;
+  uint32_t bf_smem_bytes;
+  uint32_t group_smem_cap;    // groups kept in shared memory when n_groups <= this
+  uint32_t q1_cap, q2_cap;    // power-of-two survivor ring sizes
+  uint32_t reorder_period;    // chunks between adaptive re-rankings
+  uint32_t smem_bytes;        // total dynamic shared memory
+};
+
+// Slot of key k: (k - key_min) mod ht_len, computed as an unsigned 32-bit
+// offset (HASH, crystal/join.cuh:27).  In-range keys take the subtraction
+// only; others use Lemire-Kaser-Kurz direct remainder with M = ceil(2^64/d).
+__host__ __device__ __forceinline__ uint32_t slot_of(int32_t k, int32_t kmin, uint32_t len, uint64_t m) {
+  uint32_t d = (uint32_t)k - (uint32_t)kmin;
+  if (d < len) return d;
+#ifdef __CUDA_ARCH__
+  uint64_t low = m * (uint64_t)d;
+  return (uint32_t)__umul64hi(low, (uint64_t)len);
+#else
+  return d % len;
+#endif
+}
+
+// Register-blocked filter geometry of PHT slot s: one 64-bit word, chosen by the
+// top bits of a Fibonacci multiplicative hash (Knuth, TAOCP vol. 3, 6.4), and a
+// mask of k bits whose positions are 6-bit fields from the top of a second,
+// independent multiplicative hash.  Keying on the slot (not the raw key) makes
+// the filter agree with the PHT: it never rejects a row whose slot is occupied.
+__host__ __device__ __forceinline__ uint32_t bf_word(uint32_t slot, uint32_t log2w) {
+  return log2w ? ((slot * 0x9E3779B1u) >> (32 - log2w)) : 0u;
+}
+__host__ __device__ __forceinline__ uint64_t bf_mask(uint32_t slot, uint32_t k) {
+  const uint32_t g = slot * 0x85EBCA77u;
+  uint64_t m = 1ull << (g >> 26);
+  if (k > 1) m |= 1ull << ((g >> 20) & 63u);
+  if (k > 2) m |= 1ull << ((g >> 14) & 63u);
+  if (k > 3) m |= 1ull << ((g >> 8) & 63u);
+  return m;
+}
+
+__host__ __device__ __forceinline__ uint32_t ceil_log2(uint64_t x) {
+  uint32_t l = 0;
+  while ((1ull << l) < x) ++l;
+  return l;
+}
+
+// Filter geometry chosen from the number of inserted keys (blocked layout):
+// 64-bit words = next power of two of ceil(n * bits_per_key / 64), clamped.
+__host__ __device__ __forceinline__ uint32_t bf_blocked_log2(uint64_t n_inserted, uint32_t bits_per_key,
+                                                             uint32_t max_log2) {
+  uint64_t bits = n_inserted * (uint64_t)bits_per_key;
+  uint64_t words = (bits + 63) / 64;
+  if (words < 1) words = 1;
+  uint32_t l = ceil_log2(words);
+  return l > max_log2 ? max_log2 : l;
+}
+
+}  // namespace sj

@@ -1,0 +1,389 @@
+"""ctypes binding of the star-join engine's C ABI (include/starjoin.h).
+
+Host-side harness for tests and benchmarks: loads the in-tree
+_build/libstarjoin.so, mirrors the ABI structs, and offers helpers to describe
+the star-schema workloads (synthetic columns with the reference's SSB shapes) and
+queries (Q3.3 of src/ssb-jo/q33/*.cu, and its 4-dimension / variable-selectivity
+forms).  Device buffers are torch CUDA tensors (plumbing only); every kernel that
+computes the join is the engine's own CUDA code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import os
+from typing import Any, Dict, List, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libstarjoin.so")
+
+MAX_DIMS = 4
+MAX_IN_CODES = 4096
+
+SJ_OK = 0
+SJ_ERR_INVALID_ARGUMENT = 1
+SJ_ERR_UNSUPPORTED = 2
+SJ_ERR_OUT_OF_MEMORY = 3
+SJ_ERR_CUDA = 4
+SJ_ERR_CAPACITY = 5
+SJ_ERR_TIMEOUT = 6
+SJ_ERR_NO_DEVICE = 7
+SJ_ERR_REJECTED = 8
+
+PRED_ALL, PRED_IN, PRED_RANGE = 0, 1, 2
+
+# generator column ids / kinds (csrc/sj_datagen.h)
+COL_FK_CUST, COL_FK_SUPP, COL_FK_PART, COL_FK_DATE, COL_REVENUE, COL_SUPPLYCOST = 1, 2, 3, 4, 5, 6
+COL_CUST_CITY, COL_CUST_SEL = 11, 12
+COL_SUPP_CITY, COL_SUPP_SEL = 21, 22
+COL_PART_CATEGORY, COL_PART_SEL = 31, 32
+COL_DATE_SEL = 42
+GEN_UNIFORM, GEN_DATEKEY, GEN_SEQ, GEN_DATE_SEQ, GEN_DATE_YEAR = 0, 1, 2, 3, 4
+DATE_DAYS, DATE_MIN, DATE_MAX = 2556, 19920101, 19981230
+
+
+class StarJoinError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class SjDim(C.Structure):
+    _fields_ = [
+        ("fact_fk", C.c_void_p), ("key", C.c_void_p), ("filter_attr", C.c_void_p),
+        ("payload", C.c_void_p), ("rows", C.c_int64), ("key_min", C.c_int32),
+        ("ht_len", C.c_int32), ("pred_kind", C.c_int32), ("pred_lo", C.c_int32),
+        ("pred_hi", C.c_int32), ("in_count", C.c_int32), ("in_codes", C.c_void_p),
+        ("group", C.c_int32), ("payload_min", C.c_int32), ("payload_max", C.c_int32),
+    ]
+
+
+class SjTuning(C.Structure):
+    _fields_ = [("threads", C.c_int32), ("chunk_rows", C.c_int32), ("stages", C.c_int32),
+                ("ctas_per_sm", C.c_int32), ("compact_threshold", C.c_int32),
+                ("bf_smem_bytes", C.c_int32)]
+
+
+class SjPlan(C.Structure):
+    _fields_ = [
+        ("n_dims", C.c_int32), ("dims", SjDim * MAX_DIMS), ("measure", C.c_void_p),
+        ("measure_sub", C.c_void_p), ("fact_rows", C.c_int64), ("row_begin", C.c_int64),
+        ("row_end", C.c_int64), ("order", C.c_int32 * MAX_DIMS), ("lip", C.c_int32),
+        ("adaptive", C.c_int32), ("bf_bits_per_key", C.c_int32), ("bf_hashes", C.c_int32),
+        ("tune", SjTuning),
+    ]
+
+
+class SjGroupRow(C.Structure):
+    _fields_ = [("attr", C.c_int32 * MAX_DIMS), ("count", C.c_uint64), ("sum", C.c_uint64)]
+
+
+class SjQueryStats(C.Structure):
+    _fields_ = [
+        ("rows_scanned", C.c_uint64), ("step_in", C.c_uint64 * 8), ("step_out", C.c_uint64 * 8),
+        ("bf_inserted", C.c_uint64 * MAX_DIMS), ("bf_words", C.c_uint64 * MAX_DIMS),
+        ("groups", C.c_uint64), ("reorders", C.c_uint64), ("error_flags", C.c_uint32),
+        ("build_ms", C.c_float), ("probe_ms", C.c_float),
+    ]
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def load(build_if_missing: bool = True) -> C.CDLL:
+    """Load the engine library (building it with nvcc when absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if not build_if_missing:
+            raise FileNotFoundError(LIB_PATH)
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("sj_build_recipe", os.path.join(HERE, "build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)  # type: ignore[union-attr]
+        mod.build_engine()
+    lib = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    sig = {
+        "sj_engine_create": (C.c_int, [C.c_int, C.POINTER(P)]),
+        "sj_engine_destroy": (None, [P]),
+        "sj_status_string": (C.c_char_p, [C.c_int]),
+        "sj_last_error": (C.c_char_p, []),
+        "sj_device_sm_count": (C.c_int, [P]),
+        "sj_query_prepare": (C.c_int, [P, C.POINTER(SjPlan), C.POINTER(P)]),
+        "sj_query_build": (C.c_int, [P, P]),
+        "sj_query_probe": (C.c_int, [P, P]),
+        "sj_query_fetch": (C.c_int, [P, C.POINTER(SjGroupRow), C.c_int64, C.POINTER(C.c_int64), P]),
+        "sj_query_get_stats": (C.c_int, [P, C.POINTER(SjQueryStats)]),
+        "sj_query_release": (None, [P]),
+        "sj_run_plain": (C.c_int, [P, C.POINTER(SjPlan), C.c_int, C.POINTER(SjGroupRow), C.c_int64,
+                                   C.POINTER(C.c_int64), C.POINTER(C.c_float), P]),
+        "sj_ssb_q33_run": (C.c_int, [P] + [P] * 4 + [C.c_int64] + [P] * 2 + [C.c_int64] + [P] * 2 +
+                           [C.c_int64] + [P] * 2 + [C.c_int64] + [P, C.c_int32, C.c_int32,
+                                                                 C.POINTER(SjGroupRow), C.c_int64,
+                                                                 C.POINTER(C.c_int64),
+                                                                 C.POINTER(C.c_float)]),
+        "sj_bloom_test": (C.c_int, [P, P, C.c_int64, P, P, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                                    C.c_int32, P]),
+        "sj_gen_column_device": (C.c_int, [P, C.c_int64, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
+                                           C.c_int32, P]),
+        "sj_gen_column_host": (None, [P, C.c_int64, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
+                                      C.c_int32, C.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_symbols() -> List[str]:
+    """Entry points declared in include/starjoin.h that the library must export."""
+    return [
+        "sj_engine_create", "sj_engine_destroy", "sj_status_string", "sj_last_error",
+        "sj_device_sm_count", "sj_query_prepare", "sj_query_build", "sj_query_probe",
+        "sj_query_fetch", "sj_query_get_stats", "sj_query_release", "sj_run_plain",
+        "sj_ssb_q33_run", "sj_bloom_test", "sj_gen_column_device", "sj_gen_column_host",
+    ]
+
+
+def check(status: int) -> None:
+    if status != SJ_OK:
+        lib = load()
+        raise StarJoinError(status, lib.sj_last_error().decode(errors="replace"))
+
+
+# ---------------------------------------------------------------- workload ----
+@dataclasses.dataclass(frozen=True)
+class StarSchema:
+    """Sizes and seed of a synthetic star schema (BASE distributions of SSB Q3.x)."""
+    seed: int
+    fact_rows: int
+    cust_rows: int
+    supp_rows: int
+    part_rows: int = 0
+    date_rows: int = DATE_DAYS
+
+    def column_specs(self) -> Dict[str, tuple]:
+        """name -> (length, column id, kind, lo, hi)."""
+        n = self.fact_rows
+        specs = {
+            "fk_cust": (n, COL_FK_CUST, GEN_UNIFORM, 1, self.cust_rows),
+            "fk_supp": (n, COL_FK_SUPP, GEN_UNIFORM, 1, self.supp_rows),
+            "fk_date": (n, COL_FK_DATE, GEN_DATEKEY, 0, 0),
+            "revenue": (n, COL_REVENUE, GEN_UNIFORM, 1, 10_000_000),
+            "c_key": (self.cust_rows, 0, GEN_SEQ, 1, 0),
+            "c_city": (self.cust_rows, COL_CUST_CITY, GEN_UNIFORM, 0, 249),
+            "c_sel": (self.cust_rows, COL_CUST_SEL, GEN_UNIFORM, 0, 999),
+            "s_key": (self.supp_rows, 0, GEN_SEQ, 1, 0),
+            "s_city": (self.supp_rows, COL_SUPP_CITY, GEN_UNIFORM, 0, 249),
+            "s_sel": (self.supp_rows, COL_SUPP_SEL, GEN_UNIFORM, 0, 999),
+            "d_key": (self.date_rows, 0, GEN_DATE_SEQ, 0, 0),
+            "d_year": (self.date_rows, 0, GEN_DATE_YEAR, 0, 0),
+            "d_sel": (self.date_rows, COL_DATE_SEL, GEN_UNIFORM, 0, 999),
+        }
+        if self.part_rows:
+            specs.update({
+                "fk_part": (n, COL_FK_PART, GEN_UNIFORM, 1, self.part_rows),
+                "supplycost": (n, COL_SUPPLYCOST, GEN_UNIFORM, 1, 100_000),
+                "p_key": (self.part_rows, 0, GEN_SEQ, 1, 0),
+                "p_category": (self.part_rows, COL_PART_CATEGORY, GEN_UNIFORM, 0, 24),
+                "p_sel": (self.part_rows, COL_PART_SEL, GEN_UNIFORM, 0, 999),
+            })
+        return specs
+
+
+def gen_host(schema: StarSchema, names: Optional[Sequence[str]] = None, threads: int = 0) -> Dict[str, np.ndarray]:
+    """Generate columns on the host (no GPU needed)."""
+    lib = load()
+    out = {}
+    for name, (n, col, kind, lo, hi) in schema.column_specs().items():
+        if names is not None and name not in names:
+            continue
+        a = np.empty(max(n, 0), dtype=np.int32)
+        lib.sj_gen_column_host(a.ctypes.data, n, schema.seed, col, kind, lo, hi, threads)
+        out[name] = a
+    return out
+
+
+def gen_device(schema: StarSchema, names: Optional[Sequence[str]] = None, device: int = 0):
+    """Generate columns directly into torch CUDA tensors (same values as gen_host)."""
+    import torch
+    lib = load()
+    out = {}
+    for name, (n, col, kind, lo, hi) in schema.column_specs().items():
+        if names is not None and name not in names:
+            continue
+        t = torch.empty(max(n, 1), dtype=torch.int32, device=f"cuda:{device}")[:n]
+        check(lib.sj_gen_column_device(t.data_ptr(), n, schema.seed, col, kind, lo, hi, None))
+        out[name] = t
+    return out
+
+
+# ------------------------------------------------------------------ queries ----
+def q33_query(schema: StarSchema, order=(0, 1, 2), lip=True, bf_bits_per_key=0, bf_hashes=2,
+              adaptive=False, cities=(231, 235), row_range=None) -> Dict[str, Any]:
+    """SSB Q3.3 as the reference drivers run it (src/ssb-jo/q33/0-lip.cu:114-203):
+    dims 0 = supplier (s_city IN cities), 1 = customer (c_city IN cities),
+    2 = date (d_year <= 1997, key-range table of 61130 slots from 19920101);
+    group by (s_city, c_city, d_year); SUM(revenue)."""
+    return {
+        "dims": [
+            {"fk": "fk_supp", "key": "s_key", "attr": "s_city", "payload": "s_city", "key_min": 0,
+             "ht_len": schema.supp_rows, "pred": ("in", list(cities)), "group": True,
+             "payload_range": (0, 249)},
+            {"fk": "fk_cust", "key": "c_key", "attr": "c_city", "payload": "c_city", "key_min": 0,
+             "ht_len": schema.cust_rows, "pred": ("in", list(cities)), "group": True,
+             "payload_range": (0, 249)},
+            {"fk": "fk_date", "key": "d_key", "attr": "d_year", "payload": "d_year",
+             "key_min": DATE_MIN, "ht_len": DATE_MAX - DATE_MIN + 1,
+             "pred": ("range", -(2 ** 31), 1997), "group": True, "payload_range": (1992, 1998)},
+        ],
+        "measure": "revenue", "measure_sub": None,
+        "row_range": row_range if row_range is not None else (0, schema.fact_rows),
+        "order": list(order), "lip": bool(lip), "adaptive": bool(adaptive),
+        "bf_bits_per_key": int(bf_bits_per_key), "bf_hashes": int(bf_hashes),
+    }
+
+
+def fill_plan(query: Dict[str, Any], cols: Dict[str, Any], fact_rows: int, tune: Optional[dict] = None):
+    """Translate a query description into an SjPlan over device columns.
+    Returns (plan, keepalive) -- keepalive holds ctypes arrays the plan points to."""
+    def ptr(name):
+        if name is None:
+            return None
+        t = cols[name]
+        return t.data_ptr() if hasattr(t, "data_ptr") else t.ctypes.data
+
+    def nrows(name):
+        return int(cols[name].shape[0])
+
+    plan = SjPlan()
+    keep = []
+    dims = query["dims"]
+    plan.n_dims = len(dims)
+    for i, d in enumerate(dims):
+        sd = plan.dims[i]
+        sd.fact_fk = ptr(d["fk"])
+        sd.key = ptr(d["key"])
+        sd.filter_attr = ptr(d.get("attr"))
+        sd.payload = ptr(d.get("payload"))
+        sd.rows = nrows(d["key"])
+        sd.key_min = int(d.get("key_min", 0))
+        sd.ht_len = int(d["ht_len"])
+        pred = d.get("pred", ("all",))
+        if pred[0] == "in":
+            codes = (C.c_int32 * max(1, len(pred[1])))(*pred[1])
+            keep.append(codes)
+            sd.pred_kind, sd.in_count, sd.in_codes = PRED_IN, len(pred[1]), C.addressof(codes)
+        elif pred[0] == "range":
+            sd.pred_kind, sd.pred_lo, sd.pred_hi = PRED_RANGE, int(pred[1]), int(pred[2])
+        else:
+            sd.pred_kind = PRED_ALL
+        sd.group = 1 if d.get("group") else 0
+        if d.get("group"):
+            sd.payload_min, sd.payload_max = d["payload_range"]
+    plan.measure = ptr(query["measure"])
+    plan.measure_sub = ptr(query.get("measure_sub"))
+    plan.fact_rows = fact_rows
+    plan.row_begin, plan.row_end = query["row_range"]
+    for i, o in enumerate(query["order"]):
+        plan.order[i] = o
+    plan.lip = 1 if query["lip"] else 0
+    plan.adaptive = 1 if query.get("adaptive") else 0
+    plan.bf_bits_per_key = query.get("bf_bits_per_key", 0)
+    plan.bf_hashes = query.get("bf_hashes", 2)
+    if tune:
+        for k, v in tune.items():
+            setattr(plan.tune, k, int(v))
+    return plan, keep
+
+
+def rows_to_list(rows, n: int, query: Dict[str, Any]) -> List[tuple]:
+    """Result rows as sorted tuples (grouped attrs in dim order..., count, sum)."""
+    gdims = [i for i, d in enumerate(query["dims"]) if d.get("group")]
+    out = []
+    for r in rows[:n]:
+        out.append(tuple(int(r.attr[i]) for i in gdims) + (int(r.count), int(r.sum)))
+    return sorted(out)
+
+
+class Engine:
+    """One engine handle on one device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        check(self.lib.sj_engine_create(device, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            self.lib.sj_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def sm_count(self) -> int:
+        return int(self.lib.sj_device_sm_count(self.h))
+
+    def run(self, query, cols, fact_rows, host_columns=False, tune=None, cap=1 << 20, stream=None):
+        """Run one query end to end (sj_run_plain); returns (rows, ms)."""
+        plan, keep = fill_plan(query, cols, fact_rows, tune)
+        rows = (SjGroupRow * cap)()
+        n = C.c_int64()
+        ms = C.c_float()
+        check(self.lib.sj_run_plain(self.h, C.byref(plan), 1 if host_columns else 0, rows, cap, C.byref(n),
+                                    C.byref(ms), stream))
+        return rows_to_list(rows, n.value, query), ms.value
+
+    def prepare(self, query, cols, fact_rows, tune=None) -> "Query":
+        plan, keep = fill_plan(query, cols, fact_rows, tune)
+        h = C.c_void_p()
+        check(self.lib.sj_query_prepare(self.h, C.byref(plan), C.byref(h)))
+        return Query(self, h, query, keep, cols)
+
+
+class Query:
+    """A prepared query: build/probe can be re-run (device state is reused)."""
+
+    def __init__(self, eng: Engine, h, query, keep, cols):
+        self.eng, self.h, self.query, self._keep, self._cols = eng, h, query, keep, cols
+
+    def build(self, stream=None):
+        check(self.eng.lib.sj_query_build(self.h, stream))
+
+    def probe(self, stream=None):
+        check(self.eng.lib.sj_query_probe(self.h, stream))
+
+    def fetch(self, cap=1 << 20, stream=None):
+        rows = (SjGroupRow * cap)()
+        n = C.c_int64()
+        check(self.eng.lib.sj_query_fetch(self.h, rows, cap, C.byref(n), stream))
+        return rows_to_list(rows, n.value, self.query)
+
+    def stats(self) -> SjQueryStats:
+        s = SjQueryStats()
+        check(self.eng.lib.sj_query_get_stats(self.h, C.byref(s)))
+        return s
+
+    def release(self):
+        if self.h:
+            self.eng.lib.sj_query_release(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass

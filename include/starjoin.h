@@ -1,0 +1,213 @@
+/*
+ * starjoin.h -- C ABI of the B200 star-join engine (sm_100a).
+ *
+ * One query = a streaming scan of int32 fact columns, per-dimension Bloom
+ * pre-filters applied in Lookahead-Information-Passing (LIP) order, probes into
+ * selective perfect hash tables (PHTs) built from the filtered dimension
+ * tables, and an exact uint64 group-by SUM.
+ *
+ * Reference interfaces this ABI replaces (yliang412/crystal-opt):
+ *   - runQuery(...)            src/ssb-jo/q33/0-lip.cu:205-302 (LIP drivers) and
+ *                              src/ssb-jo/q33/0-naive.cu:178-257 (naive drivers):
+ *                              alloc -> memset -> dimension builds -> probe -> D2H.
+ *                              Replaced by sj_run_plain() / sj_ssb_q33_run().
+ *   - build_hashtable_{s,c,d} src/ssb-jo/q33/0-lip.cu:114-203 (predicate ->
+ *                              BlockBuildBloomFilter -> BlockBuildSelectivePHT_2).
+ *                              Replaced by sj_query_build().
+ *   - probe<128,4>             src/ssb-jo/q33/0-lip.cu:28-112 (BF probes in LIP
+ *                              order, PHT probes, group atomicAdd).
+ *                              Replaced by sj_query_probe().
+ *   - the reference's Q4.1 4-dimension LIP driver (src/ssb-jo/q41/0-lip.cu:28-131)
+ *                              is the n_dims == 4 form of the same plan.
+ *
+ * Conventions
+ *   - Every entry point returns an sj_status; nothing calls exit() (the
+ *     reference aborts through CubDebugExit, src/ssb-jo/q33/0-lip.cu:224-242).
+ *     sj_last_error() gives a human-readable detail for the calling thread.
+ *   - Column pointers are caller-owned.  Unless a call says otherwise they are
+ *     device pointers, int32, 16-byte aligned (cudaMalloc gives 256).
+ *   - Streams are passed as `void*` holding a cudaStream_t (NULL = legacy
+ *     default stream, as the reference uses).
+ *   - Handles are not shared between threads without external locking; distinct
+ *     handles may be used concurrently.
+ *   - Key hashing follows the reference exactly: a dimension key K occupies PHT
+ *     slot (K - key_min) mod ht_len (crystal/join.cuh:27, HASH).  Keys below
+ *     key_min are reduced as unsigned 32-bit offsets (the reference would index
+ *     out of bounds there).
+ */
+#ifndef STARJOIN_H
+#define STARJOIN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SJ_MAX_DIMS 4
+#define SJ_MAX_IN_CODES 4096   /* IN-list predicates: codes in [0, 4096) */
+#define SJ_MAX_PAYLOAD_SPAN 65536 /* payload_max - payload_min + 1 for grouped dims */
+
+typedef enum sj_status {
+  SJ_OK = 0,
+  SJ_ERR_INVALID_ARGUMENT = 1,
+  SJ_ERR_UNSUPPORTED = 2,
+  SJ_ERR_OUT_OF_MEMORY = 3,
+  SJ_ERR_CUDA = 4,
+  SJ_ERR_CAPACITY = 5,   /* caller's result buffer is too small; *n_out holds the need */
+  SJ_ERR_TIMEOUT = 6,    /* a bounded device-side wait expired; context stays usable */
+  SJ_ERR_NO_DEVICE = 7,  /* no CUDA device / extension built without one */
+  SJ_ERR_REJECTED = 8    /* admission control refused the request (serving form) */
+} sj_status;
+
+/* Dimension predicate kinds (the reference's BlockPred* chains in the build
+ * kernels, src/ssb-jo/q33/0-lip.cu:130-135 and :187-190). */
+typedef enum sj_pred_kind {
+  SJ_PRED_ALL = 0,   /* every row qualifies (InitFlags) */
+  SJ_PRED_IN = 1,    /* attr IN {codes}   (BlockPredEQ + BlockPredOrEQ ...) */
+  SJ_PRED_RANGE = 2  /* lo <= attr <= hi (BlockPredGTE / BlockPredLTE) */
+} sj_pred_kind;
+
+typedef struct sj_dim {
+  /* fact side */
+  const int32_t* fact_fk;     /* fact foreign-key column (fact_rows entries) */
+  /* dimension table (rows entries per column) */
+  const int32_t* key;         /* primary key column (e.g. s_suppkey) */
+  const int32_t* filter_attr; /* attribute tested by the predicate (e.g. s_city) */
+  const int32_t* payload;     /* value stored in the PHT and used as group key
+                                 (e.g. s_city, d_year); NULL -> key-only table
+                                 (BlockBuildSelectivePHT_1 form) */
+  int64_t rows;
+  int32_t key_min;            /* keys_min of HASH (19920101 for the date table) */
+  int32_t ht_len;             /* PHT slots (reference: dim rows, or
+                                 19981230-19920101+1 = 61130 for dates) */
+  int32_t pred_kind;          /* sj_pred_kind */
+  int32_t pred_lo, pred_hi;   /* SJ_PRED_RANGE bounds (inclusive) */
+  int32_t in_count;           /* SJ_PRED_IN: number of codes */
+  const int32_t* in_codes;    /* SJ_PRED_IN: HOST array of codes in [0, SJ_MAX_IN_CODES) */
+  int32_t group;              /* 1: payload is part of the group-by key */
+  int32_t payload_min;        /* grouped dims: payload domain [min, max] */
+  int32_t payload_max;
+} sj_dim;
+
+/* Launch geometry; 0 fields are chosen by the engine (or the autotuner cache). */
+typedef struct sj_tuning {
+  int32_t threads;            /* threads per CTA of the probe kernel (128..1024) */
+  int32_t chunk_rows;         /* fact rows per TMA stage (multiple of 4*threads) */
+  int32_t stages;             /* TMA ring depth (2..8) */
+  int32_t ctas_per_sm;        /* persistent CTAs per SM (1..4) */
+  int32_t compact_threshold;  /* survivors queued before a compaction round (0 = threads) */
+  int32_t bf_smem_bytes;      /* shared-memory budget for Bloom filters */
+} sj_tuning;
+
+typedef struct sj_plan {
+  int32_t n_dims;                 /* 1..SJ_MAX_DIMS */
+  sj_dim dims[SJ_MAX_DIMS];
+  const int32_t* measure;         /* SUM(measure) (e.g. lo_revenue) */
+  const int32_t* measure_sub;     /* optional: SUM(measure - measure_sub) (Q4.x) */
+  int64_t fact_rows;              /* length of every fact column */
+  int64_t row_begin;              /* scanned range [row_begin, row_end) */
+  int64_t row_end;                /* -1 -> fact_rows */
+  int32_t order[SJ_MAX_DIMS];     /* join order: dim indices, first = outermost */
+  int32_t lip;                    /* 1: all Bloom probes first (LIP), 0: naive */
+  int32_t adaptive;               /* 1: re-rank the LIP order from observed pass rates */
+  int32_t bf_bits_per_key;        /* 0: direct bitmap, one bit per key slot
+                                     (crystal/bloom.cuh layout); >0: register-blocked
+                                     filter with this many bits per inserted key */
+  int32_t bf_hashes;              /* blocked filter: bits set per key in one 64-bit word (1..4) */
+  sj_tuning tune;
+} sj_plan;
+
+/* One result group.  attr[d] is the payload of dimension d when that dimension
+ * is grouped, else 0.  sum is the two's-complement uint64 sum of the measure
+ * (the reference's uint64 accumulation, src/ssb-jo/q31/0-lip.cu:102-110);
+ * its low 32 bits equal the reference's int32 sums of Q3.3
+ * (src/ssb-jo/q33/0-lip.cu:108). */
+typedef struct sj_group_row {
+  int32_t attr[SJ_MAX_DIMS];
+  uint64_t count;
+  uint64_t sum;
+} sj_group_row;
+
+/* Per-query counters read back after a probe. */
+typedef struct sj_query_stats {
+  uint64_t rows_scanned;
+  uint64_t step_in[2 * SJ_MAX_DIMS];   /* rows entering plan step i */
+  uint64_t step_out[2 * SJ_MAX_DIMS];  /* rows leaving plan step i */
+  uint64_t bf_inserted[SJ_MAX_DIMS];   /* keys inserted into each dimension's filter */
+  uint64_t bf_words[SJ_MAX_DIMS];      /* filter size in 32-bit words */
+  uint64_t groups;                     /* non-empty groups */
+  uint64_t reorders;                   /* adaptive LIP re-rankings (all CTAs) */
+  uint32_t error_flags;                /* device-side error bits (0 = none) */
+  float build_ms, probe_ms;            /* CUDA-event times of the last run */
+} sj_query_stats;
+
+typedef struct sj_engine sj_engine;
+typedef struct sj_query sj_query;
+
+/* ---- engine ------------------------------------------------------------ */
+sj_status sj_engine_create(int device, sj_engine** out);
+void sj_engine_destroy(sj_engine* e);
+const char* sj_status_string(sj_status s);
+const char* sj_last_error(void);
+int sj_device_sm_count(sj_engine* e);
+
+/* ---- plain single query (drop-in for runQuery) ------------------------- */
+/* Validate the plan and reserve device state (PHTs, filters, groups). */
+sj_status sj_query_prepare(sj_engine* e, const sj_plan* plan, sj_query** out);
+/* Dimension builds: predicate -> filter insert -> PHT insert (async on stream). */
+sj_status sj_query_build(sj_query* q, void* stream);
+/* Fused scan -> LIP filters -> PHT probes -> group SUM (async on stream). */
+sj_status sj_query_probe(sj_query* q, void* stream);
+/* Wait for the stream, copy the groups out (sorted by the grouped attrs in
+ * dimension order).  SJ_ERR_CAPACITY if cap < groups (*n_out = groups). */
+sj_status sj_query_fetch(sj_query* q, sj_group_row* out, int64_t cap, int64_t* n_out, void* stream);
+sj_status sj_query_get_stats(sj_query* q, sj_query_stats* out);
+void sj_query_release(sj_query* q);
+
+/* prepare + build + probe + fetch + release in one call; *ms gets the CUDA-event
+ * time from the first build launch to the end of the probe (the span the
+ * reference's time_query covers, src/ssb-jo/q33/0-lip.cu:216-278).
+ * If host_columns is nonzero every column pointer in the plan is HOST memory:
+ * the engine stages the fact columns to the device itself, inside *ms. */
+sj_status sj_run_plain(sj_engine* e, const sj_plan* plan, int host_columns,
+                       sj_group_row* out, int64_t cap, int64_t* n_out, float* ms, void* stream);
+
+/* The reference's Q3.3 call, argument for argument (src/ssb-jo/q33/0-lip.cu:205):
+ * predicates s_city IN {231,235}, c_city IN {231,235}, d_year <= 1997, group by
+ * (d_year, c_city, s_city), SUM(lo_revenue).  order[3] lists the join order
+ * over {0 = supplier, 1 = customer, 2 = date} (the six drivers
+ * src/ssb-jo/q33/{0..5}-{lip,naive}.cu); lip selects the LIP or naive driver;
+ * bf_bits_per_key = 0 keeps the reference's direct bitmap filter.
+ * Rows come back as attr[0] = s_city, attr[1] = c_city, attr[2] = d_year. */
+sj_status sj_ssb_q33_run(sj_engine* e,
+                         const int32_t* lo_orderdate, const int32_t* lo_custkey,
+                         const int32_t* lo_suppkey, const int32_t* lo_revenue, int64_t lo_len,
+                         const int32_t* d_datekey, const int32_t* d_year, int64_t d_len,
+                         const int32_t* s_suppkey, const int32_t* s_city, int64_t s_len,
+                         const int32_t* c_custkey, const int32_t* c_city, int64_t c_len,
+                         const int32_t order[3], int32_t lip, int32_t bf_bits_per_key,
+                         sj_group_row* out, int64_t cap, int64_t* n_out, float* time_query_ms);
+
+/* ---- Bloom filter unit interface (tests; the reference's src/ops/bloom.cu) -- */
+/* Build a filter over keys[flags != 0] and probe probe_keys; out_flags[i] = 1 if
+ * probe_keys[i] may be present.  All pointers are device pointers.
+ * bits_per_key = 0 selects the direct bitmap of `direct_words` 32-bit words. */
+sj_status sj_bloom_test(const int32_t* keys, const int32_t* flags, int64_t n_keys,
+                        const int32_t* probe_keys, int32_t* out_flags, int64_t n_probe,
+                        int32_t bits_per_key, int32_t hashes, int32_t key_min,
+                        int32_t direct_words, void* stream);
+
+/* ---- synthetic data on the device (same values as the host generator) ---- */
+/* Fill dst[0..n) with generated column values (see sj_datagen.h kinds). */
+sj_status sj_gen_column_device(int32_t* dst, int64_t n, uint64_t seed, int32_t col,
+                               int32_t kind, int32_t lo, int32_t hi, void* stream);
+/* Host form of the same generator (needs no GPU); threads <= 0 uses all cores. */
+void sj_gen_column_host(int32_t* dst, int64_t n, uint64_t seed, int32_t col,
+                        int32_t kind, int32_t lo, int32_t hi, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STARJOIN_H */

@@ -1,0 +1,94 @@
+"""Compile the reference's own SSB Q3.3 drivers into oracle/_ref/ -- TEST INFRASTRUCTURE.
+
+The driver sources are compiled where they lie under the reference tree
+(default /root/reference, override with CRYSTAL_OPT_REF); nothing is copied.
+Each binary is one driver (src/ssb-jo/q33/<order>-<lip|naive>.cu) wrapped by
+ref_runner.cu, which supplies main() and the synthetic columns.  The reference's
+CUB 1.6.4 test header is replaced by ref_shim/cub/test/test_util.h.  Flags follow
+the reference Makefile (-O3 -lineinfo -Xptxas -dlcm=ca, Makefile:23,35) with the
+architecture switched to sm_100a.
+
+The binaries need a GPU to run; they travel with the repository snapshot.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+REF = os.environ.get("CRYSTAL_OPT_REF", "/root/reference")
+ORDERS = range(6)
+METHODS = ("lip", "naive")
+
+
+def binary(order: int, method: str) -> str:
+    return os.path.join(OUT, f"q33_{order}_{method}")
+
+
+def available() -> bool:
+    return os.path.isdir(os.path.join(REF, "src", "ssb-jo", "q33"))
+
+
+def _compile(order: int, method: str) -> str:
+    src = os.path.join(REF, "src", "ssb-jo", "q33", f"{order}-{method}.cu")
+    out = binary(order, method)
+    deps = [src, os.path.join(HERE, "ref_runner.cu"), os.path.join(HERE, "ref_shim", "cub", "test", "test_util.h")]
+    if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
+        return out
+    cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+           "-Xptxas", "-dlcm=ca", "-I", REF, "-I", os.path.join(HERE, "ref_shim"),
+           f'-DREF_DRIVER="{src}"', f"-DREF_LIP={1 if method == 'lip' else 0}",
+           "-o", out + ".tmp", os.path.join(HERE, "ref_runner.cu")]
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
+    os.replace(out + ".tmp", out)
+    return out
+
+
+def build(jobs: int = 0) -> list[str]:
+    """Build all 12 drivers (skipped when the reference tree is absent)."""
+    if not available():
+        return []
+    os.makedirs(OUT, exist_ok=True)
+    jobs = jobs or min(8, os.cpu_count() or 1)
+    with cf.ThreadPoolExecutor(jobs) as ex:
+        futs = [ex.submit(_compile, o, m) for o in ORDERS for m in METHODS]
+        return [f.result() for f in futs]
+
+
+def parse_output(text: str) -> dict:
+    """Parse a runner's stdout: result groups (year, c_city, s_city, int32 sum),
+    time_query values and probe-only times."""
+    import json
+    groups = []
+    times, probe = [], []
+    in_res = False
+    for line in text.splitlines():
+        line = line.strip()
+        if line == "Result:":
+            in_res, groups = True, []
+            continue
+        if line.startswith("Res Count:"):
+            in_res = False
+            continue
+        if in_res:
+            parts = line.split()
+            if len(parts) == 4:
+                groups.append(tuple(int(x) for x in parts))
+            continue
+        if line.startswith("{"):
+            rec = json.loads(line)
+            if "time_query" in rec:
+                times.append(rec["time_query"])
+            if "probe_ms" in rec:
+                probe.append(rec["probe_ms"])
+    return {"groups": sorted(groups), "time_query_ms": times, "probe_ms": probe}
+
+
+if __name__ == "__main__":
+    for p in build():
+        print(p)
+    if not available():
+        print(f"reference tree not found at {REF}", file=sys.stderr)

@@ -1,0 +1,53 @@
+"""Regenerate the golden vectors from the reference's own CUDA drivers.
+
+Runs every oracle/_ref/q33_<order>_<lip|naive> binary (the unmodified
+src/ssb-jo/q33/*.cu drivers, built by oracle/build_ref.py) on the seeded small
+star schema and records the groups each prints: (d_year, c_city, s_city, int32
+SUM(lo_revenue)).  Needs a GPU; run from the repository root:
+
+    python tests/golden/make_golden.py
+"""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+sys.path.insert(0, os.path.join(ROOT, "crystal-opt_b200"))
+
+import build_ref  # noqa: E402
+from workloads import SMALL  # noqa: E402
+
+
+def run_driver(order: int, method: str, schema, trials: int = 1, probe_trials: int = 0, timeout=600) -> dict:
+    exe = build_ref.binary(order, method)
+    cmd = [exe, f"--seed={schema.seed}", f"--n={schema.fact_rows}", f"--c={schema.cust_rows}",
+           f"--s={schema.supp_rows}", f"--t={trials}", f"--probe_t={probe_trials}"]
+    out = subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=timeout).stdout
+    return build_ref.parse_output(out)
+
+
+def main():
+    drivers = {}
+    for o in range(6):
+        for m in ("lip", "naive"):
+            drivers[f"{o}_{m}"] = run_driver(o, m, SMALL)["groups"]
+    first = drivers["0_lip"]
+    rec = {
+        "what": "groups printed by the reference's src/ssb-jo/q33 drivers on the seeded small schema",
+        "columns": ["d_year", "c_city", "s_city", "sum_int32"],
+        "schema": {"seed": SMALL.seed, "fact_rows": SMALL.fact_rows, "cust_rows": SMALL.cust_rows,
+                   "supp_rows": SMALL.supp_rows},
+        "groups": first,
+        "drivers": drivers,
+    }
+    path = os.path.join(ROOT, "tests", "golden", "q33_small_reference.json")
+    with open(path, "w") as f:
+        json.dump(rec, f, indent=1)
+    print(path, len(first), "groups")
+
+
+if __name__ == "__main__":
+    main()

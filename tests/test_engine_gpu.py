@@ -1,0 +1,238 @@
+"""GPU parity: the engine (through its C ABI) against the CPU oracle, bit-exact
+groups, counts and uint64 sums, for every join order, naive and LIP, each filter
+layout, and the edge cases the reference's kernels meet (ragged tiles, key == len,
+empty inputs)."""
+import ctypes as C
+import random
+
+import numpy as np
+import pytest
+
+from workloads import FULL, ORDERS3, REF_DRIVER_ORDERS, SMALL, columns_of, random_query, sel_query
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small(sj, torch_cuda):
+    host = sj.gen_host(SMALL)
+    dev = {k: torch_cuda.from_numpy(v).cuda() for k, v in host.items()}
+    return host, dev
+
+
+def test_device_generator_matches_host(sj, torch_cuda):
+    sc = sj.StarSchema(seed=99, fact_rows=1_000_003, cust_rows=5000, supp_rows=300, part_rows=7000)
+    host = sj.gen_host(sc)
+    dev = sj.gen_device(sc)
+    for k in host:
+        np.testing.assert_array_equal(dev[k].cpu().numpy(), host[k], k)
+
+
+@pytest.mark.parametrize("lip", [True, False])
+@pytest.mark.parametrize("order", ORDERS3)
+def test_q33_small_every_order(sj, oracle, engine, small, order, lip):
+    host, dev = small
+    q = sj.q33_query(SMALL, order=order, lip=lip)
+    want = oracle.run(q, host)
+    assert len(want) == 24
+    for bpk, k in ([(0, 1), (8, 2), (16, 3)] if lip else [(0, 1)]):
+        q["bf_bits_per_key"], q["bf_hashes"] = bpk, k
+        got, _ = engine.run(q, dev, SMALL.fact_rows)
+        assert got == want, (order, lip, bpk)
+
+
+def test_q33_reference_call_form(sj, oracle, engine, small):
+    """sj_ssb_q33_run: the reference runQuery argument list (0-lip.cu:205)."""
+    host, dev = small
+    want = oracle.run(sj.q33_query(SMALL), host)
+    for drv, order in REF_DRIVER_ORDERS.items():
+        for lip in (1, 0):
+            rows = (sj.SjGroupRow * 64)()
+            n = C.c_int64()
+            ms = C.c_float()
+            o = (C.c_int32 * 3)(*order)
+            p = lambda name: dev[name].data_ptr()
+            sj.check(engine.lib.sj_ssb_q33_run(
+                engine.h, p("fk_date"), p("fk_cust"), p("fk_supp"), p("revenue"), SMALL.fact_rows,
+                p("d_key"), p("d_year"), 2556, p("s_key"), p("s_city"), SMALL.supp_rows,
+                p("c_key"), p("c_city"), SMALL.cust_rows, o, lip, 0, rows, 64, C.byref(n), C.byref(ms)))
+            got = sorted((r.attr[0], r.attr[1], r.attr[2], r.count, r.sum) for r in rows[:n.value])
+            assert got == want, (drv, lip)
+            assert ms.value > 0
+
+
+def test_host_columns_form(sj, oracle, engine, small):
+    host, _ = small
+    q = sj.q33_query(SMALL, order=(1, 0, 2), bf_bits_per_key=16, bf_hashes=2)
+    got, ms = engine.run(q, host, SMALL.fact_rows, host_columns=True)
+    assert got == oracle.run(q, host)
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_random_queries(sj, oracle, engine, torch_cuda, seed):
+    rng = random.Random(seed)
+    sc = sj.StarSchema(seed=500 + seed % 4, fact_rows=rng.choice([1, 3, 4097, 300_001, 2_000_000]),
+                       cust_rows=rng.choice([1, 33, 30_000]), supp_rows=rng.choice([1, 2000]),
+                       part_rows=rng.choice([0, 10_000]))
+    host = sj.gen_host(sc)
+    dev = {k: torch_cuda.from_numpy(v).cuda() for k, v in host.items()}
+    for _ in range(3):
+        q = random_query(rng, sc)
+        got, _ = engine.run(q, dev, sc.fact_rows)
+        assert got == oracle.run(q, host), q
+
+
+@pytest.mark.parametrize("begin,end", [(0, 0), (5, 5), (0, 1), (1, 2), (3, 4), (1, 4096), (2, 4099),
+                                       (4095, 8193), (6_000_000 - 5, 6_000_000), (3, 6_000_000),
+                                       (1_234_567, 4_567_891)])
+def test_row_ranges_and_ragged_tails(sj, oracle, engine, small, begin, end):
+    host, dev = small
+    q = sj.q33_query(SMALL, cities=tuple(range(0, 250, 5)), row_range=(begin, end), bf_bits_per_key=8)
+    got, _ = engine.run(q, dev, SMALL.fact_rows)
+    assert got == oracle.run(q, host)
+
+
+@pytest.mark.parametrize("tune", [dict(threads=256), dict(threads=1024), dict(stages=2), dict(stages=12),
+                                  dict(chunk_rows=2048), dict(chunk_rows=16384, stages=3),
+                                  dict(bf_smem_bytes=0), dict(ctas_per_sm=2, stages=3, chunk_rows=2048)])
+def test_launch_geometry_does_not_change_results(sj, oracle, engine, small, tune):
+    host, dev = small
+    want = oracle.run(sj.q33_query(SMALL), host)
+    for lip, bpk in ((True, 16), (True, 0), (False, 0)):
+        q = sj.q33_query(SMALL, order=(2, 1, 0), lip=lip, bf_bits_per_key=bpk)
+        got, _ = engine.run(q, dev, SMALL.fact_rows, tune=tune)
+        assert got == want, (tune, lip, bpk)
+
+
+def test_no_qualifying_rows_and_all_rows(sj, oracle, engine, small):
+    host, dev = small
+    q = sj.q33_query(SMALL, cities=(250, 251))  # no city matches
+    assert engine.run(q, dev, SMALL.fact_rows)[0] == [] == oracle.run(q, host)
+    q = sj.q33_query(SMALL, cities=tuple(range(250)))
+    got, _ = engine.run(q, dev, SMALL.fact_rows)
+    assert got == oracle.run(q, host) and len(got) == 250 * 250 * 6
+
+
+def test_key_equal_to_len_and_out_of_range_fks(sj, oracle, engine, torch_cuda):
+    """FK values beyond the table alias slot (fk - min) % len, exactly as
+    BlockProbeAndPHT_2 does (crystal/join.cuh:27,123); key == len is slot 0."""
+    sc = sj.StarSchema(seed=11, fact_rows=100_000, cust_rows=97, supp_rows=13)
+    host = sj.gen_host(sc)
+    rng = np.random.default_rng(0)
+    host["fk_cust"] = rng.integers(-300, 5000, size=sc.fact_rows).astype(np.int32)
+    host["fk_supp"] = rng.integers(0, 60, size=sc.fact_rows).astype(np.int32)
+    dev = {k: torch_cuda.from_numpy(v).cuda() for k, v in host.items()}
+    for lip, bpk in ((True, 0), (True, 8), (False, 0)):
+        q = sj.q33_query(sc, cities=tuple(range(0, 250, 2)), lip=lip, bf_bits_per_key=bpk)
+        got, _ = engine.run(q, dev, sc.fact_rows)
+        assert got == oracle.run(q, host), (lip, bpk)
+
+
+def test_prepared_query_rebuild_and_reprobe(sj, oracle, engine, small):
+    host, dev = small
+    q = sj.q33_query(SMALL, order=(2, 0, 1), bf_bits_per_key=8)
+    want = oracle.run(q, host)
+    pq = engine.prepare(q, dev, SMALL.fact_rows)
+    for _ in range(3):
+        pq.build()
+        pq.probe()
+        assert pq.fetch() == want
+    st = pq.stats()
+    assert st.rows_scanned == SMALL.fact_rows
+    assert st.groups == 24
+    assert st.step_in[0] == SMALL.fact_rows
+    assert st.error_flags == 0
+    pq.release()
+
+
+def test_invalid_arguments_are_reported(sj, engine, small):
+    host, dev = small
+    q = sj.q33_query(SMALL)
+    q["order"] = [0, 0, 1]
+    with pytest.raises(sj.StarJoinError) as e:
+        engine.run(q, dev, SMALL.fact_rows)
+    assert e.value.status == sj.SJ_ERR_INVALID_ARGUMENT
+    q = sj.q33_query(SMALL)
+    q["dims"][0]["payload_range"] = (0, 100)  # s_city up to 249 falls outside
+    with pytest.raises(sj.StarJoinError) as e:
+        engine.run(q, dev, SMALL.fact_rows)
+    assert e.value.status == sj.SJ_ERR_INVALID_ARGUMENT
+    q = sj.q33_query(SMALL)
+    dev2 = dict(dev)
+    dev2["fk_supp"] = dev["fk_supp"][1:]  # 4-byte offset: not 16-byte aligned
+    with pytest.raises(sj.StarJoinError) as e:
+        engine.run(q, dev2, SMALL.fact_rows - 1)
+    assert e.value.status == sj.SJ_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("bpk", [4, 8, 16])
+@pytest.mark.parametrize("k", [1, 2, 3, 4])
+def test_bloom_no_false_negatives(sj, engine, torch_cuda, bpk, k):
+    """Every inserted key passes (the reference's bloom.cu expectation 'FN should be 0',
+    src/ops/bloom.cu:241); the false-positive rate stays near the blocked-filter bound."""
+    torch = torch_cuda
+    n = 200_000
+    keys = torch.arange(1, n + 1, dtype=torch.int32, device="cuda")
+    flags = (torch.arange(n, device="cuda") % 3 == 0).to(torch.int32)
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    sj.check(engine.lib.sj_bloom_test(keys.data_ptr(), flags.data_ptr(), n, keys.data_ptr(), out.data_ptr(), n,
+                                      bpk, k, 0, 0, None))
+    f = flags.bool()
+    assert bool(out[f].all()), "false negative"
+    fpr = out[~f].float().mean().item()
+    bound = {4: 0.45, 8: 0.2, 16: 0.06}[bpk]
+    assert fpr < bound, fpr
+
+
+def test_direct_bitmap_filter_is_exact(sj, engine, torch_cuda):
+    torch = torch_cuda
+    n = 1 << 16
+    keys = torch.arange(n, dtype=torch.int32, device="cuda") + 19920101
+    flags = (torch.arange(n, device="cuda") % 7 == 2).to(torch.int32)
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    sj.check(engine.lib.sj_bloom_test(keys.data_ptr(), flags.data_ptr(), n, keys.data_ptr(), out.data_ptr(), n,
+                                      0, 1, 19920101, n // 32, None))
+    assert torch.equal(out, flags)
+
+
+def test_four_dim_selectivity_grid(sj, oracle, engine, torch_cuda):
+    sc = sj.StarSchema(seed=77, fact_rows=3_000_000, cust_rows=60_000, supp_rows=4000, part_rows=100_000)
+    host = sj.gen_host(sc)
+    dev = {k: torch_cuda.from_numpy(v).cuda() for k, v in host.items()}
+    rng = random.Random(5)
+    for _ in range(12):
+        sels = [rng.choice([1, 10, 100, 500]) for _ in range(4)]
+        q = sel_query(sc, sels, seed=rng.randint(0, 1 << 30), order=rng.sample(range(4), 4),
+                      bpk=rng.choice([4, 8, 16]), k=rng.randint(1, 4), adaptive=rng.random() < 0.5)
+        got, _ = engine.run(q, dev, sc.fact_rows)
+        assert got == oracle.run(q, host), sels
+
+
+@pytest.fixture(scope="module")
+def full(sj, torch_cuda):
+    dev = sj.gen_device(FULL)
+    host = {k: v.cpu().numpy() for k, v in dev.items()}
+    return host, dev
+
+
+@pytest.mark.parametrize("order", [(0, 1, 2), (2, 1, 0), (1, 2, 0)])
+def test_q33_full_size(sj, oracle, engine, full, order):
+    host, dev = full
+    want = oracle.run(sj.q33_query(FULL), host)
+    assert len(want) == 24
+    for lip, bpk, adaptive in ((True, 8, False), (True, 16, True), (False, 0, False)):
+        q = sj.q33_query(FULL, order=order, lip=lip, bf_bits_per_key=bpk, adaptive=adaptive)
+        got, _ = engine.run(q, dev, FULL.fact_rows)
+        assert got == want, (order, lip, bpk, adaptive)
+
+
+def test_adaptive_lip_reorders_bad_plan(sj, engine, full):
+    host, dev = full
+    q = sj.q33_query(FULL, order=(2, 1, 0), bf_bits_per_key=16, adaptive=True)  # D first: 86% pass
+    pq = engine.prepare(q, dev, FULL.fact_rows)
+    pq.build()
+    pq.probe()
+    pq.fetch()
+    st = pq.stats()
+    assert st.reorders > 0
+    pq.release()
