@@ -60,6 +60,15 @@ def random_query(rng: random.Random, schema: sj.StarSchema, n_dims: int | None =
         dims.append({"fk": d["fk"], "key": d["key"], "attr": attr, "payload": pattr if group else None,
                      "key_min": d["key_min"], "ht_len": d["ht_len"], "pred": pred, "group": group,
                      "payload_range": (plo, phi)})
+    # keep the dense group space within the engine's 2^26 limit
+    span = 1
+    for d in dims:
+        if d["group"]:
+            w = d["payload_range"][1] - d["payload_range"][0] + 1
+            if span * w > (1 << 22):
+                d["group"], d["payload"] = False, None
+            else:
+                span *= w
     order = list(range(k))
     rng.shuffle(order)
     n = schema.fact_rows
