@@ -199,13 +199,14 @@ static sj_status validate_plan(const sj_plan* p) {
   return SJ_OK;
 }
 
-// Shrink the ring depth, then the filter budget, until the layout fits the
+// Shrink the ring depth, the chunk, then the filter budget, until the layout fits the
 // shared memory of ctas_per_sm CTAs (1 KB per CTA is reserved by the runtime).
-static void fit_geom(sj_engine* eng, SjProbeGeom& g, uint32_t ctas_per_sm) {
+static void fit_geom(sj_engine* eng, SjProbeGeom& g, uint32_t ctas_per_sm, uint32_t pass) {
   const size_t limit = std::min<size_t>(eng->smem_optin, 233472 / std::max<uint32_t>(1, ctas_per_sm) - 1024);
   g.smem_bytes = probe_smem_bytes(g);
   while (g.smem_bytes > limit) {
     if (g.stages > 2) --g.stages;
+    else if (g.chunk_rows > pass) g.chunk_rows -= pass;
     else if (g.bf_smem_bytes >= 4096) g.bf_smem_bytes /= 2;
     else if (g.bf_smem_bytes) g.bf_smem_bytes = 0;
     else if (g.group_smem_cap > 64) g.group_smem_cap /= 2;
@@ -214,36 +215,42 @@ static void fit_geom(sj_engine* eng, SjProbeGeom& g, uint32_t ctas_per_sm) {
   }
 }
 
-static void default_geom(sj_engine* eng, const sj_plan* p, SjProbeGeom& g, uint32_t& rpt) {
+// Probe launch geometry.  tune.threads is the CTA size (256, 512 or 768): one
+// producer warp plus 7, 15 or 23 consumer warps (a multiple of four warps, so the
+// register file splits evenly over the SM's four sub-partitions).  A pass covers
+// 32 * rows_per_lane rows per consumer warp; a chunk is a whole number of passes
+// of every consumer warp.
+static void default_geom(sj_engine* eng, const sj_plan* p, SjProbeGeom& g, uint32_t& rpl) {
   const sj_tuning& t = p->tune;
-  g.threads = t.threads ? (uint32_t)t.threads : 512u;
-  rpt = 4;
-  const uint32_t sb = g.threads * rpt;
-  g.chunk_rows = t.chunk_rows ? (uint32_t)t.chunk_rows : 4096u;
-  if (g.chunk_rows % sb) g.chunk_rows = (g.chunk_rows / sb + 1) * sb;
-  g.stages = t.stages ? (uint32_t)t.stages : 6u;
-  g.bf_smem_bytes = t.bf_smem_bytes ? (uint32_t)t.bf_smem_bytes : 48u * 1024u;
+  const uint32_t threads = t.threads ? (uint32_t)t.threads : 512u;
+  const uint32_t nwc = threads / 32 - 1;
+  g.threads = (nwc + 1) * 32;
+  rpl = (t.compact_threshold == 16 && nwc <= 15) ? 16u : 8u;
+  const uint32_t pass = nwc * 32 * rpl;
+  g.chunk_rows = t.chunk_rows ? (uint32_t)t.chunk_rows : 4 * pass;
+  if (g.chunk_rows % pass) g.chunk_rows = (g.chunk_rows / pass + 1) * pass;
+  g.stages = t.stages ? (uint32_t)t.stages : 2u;
+  g.bf_smem_bytes = t.bf_smem_bytes ? (uint32_t)t.bf_smem_bytes : 40u * 1024u;
   g.group_smem_cap = 1024;
   uint32_t q1 = 1;
-  while (q1 < sb + g.threads) q1 <<= 1;
+  while (q1 < 2 * 32 * rpl) q1 <<= 1;
   g.q1_cap = q1;
-  uint32_t q2 = 1;
-  while (q2 < 2 * g.threads) q2 <<= 1;
-  g.q2_cap = q2;
+  g.q2_cap = 64;
   g.reorder_period = 16;
   const uint32_t per_sm = t.ctas_per_sm ? (uint32_t)t.ctas_per_sm : 1u;
   g.grid = (uint32_t)eng->sm_count * per_sm;
-  fit_geom(eng, g, per_sm);
+  fit_geom(eng, g, per_sm, pass);
 }
 
-static sj_status check_geom(sj_engine* eng, SjProbeGeom& g, uint32_t rpt) {
-  if (g.threads != 256 && g.threads != 512 && g.threads != 1024)
-    return fail(SJ_ERR_INVALID_ARGUMENT, "threads=%u (256, 512, 1024)", g.threads);
-  if (rpt != 4 && rpt != 8 && rpt != 16) return fail(SJ_ERR_INVALID_ARGUMENT, "rows per thread %u", rpt);
-  if (g.threads == 1024 && rpt == 16) return fail(SJ_ERR_INVALID_ARGUMENT, "threads 1024 x rows 16");
+static sj_status check_geom(sj_engine* eng, SjProbeGeom& g, uint32_t rpl) {
+  const uint32_t nwc = g.threads / 32 - 1;
+  const bool ok = ((nwc == 7 || nwc == 15) && (rpl == 8 || rpl == 16)) || (nwc == 23 && (rpl == 4 || rpl == 8));
+  if (!ok) return fail(SJ_ERR_INVALID_ARGUMENT, "%u consumer warps x %u rows per lane not built", nwc, rpl);
   if (g.stages < 2 || g.stages > 16) return fail(SJ_ERR_INVALID_ARGUMENT, "stages=%u (2..16)", g.stages);
-  if (g.chunk_rows == 0 || g.chunk_rows % (g.threads * rpt) || g.chunk_rows * 4u > (1u << 19))
+  if (g.chunk_rows == 0 || g.chunk_rows % (nwc * 32 * rpl) || g.chunk_rows * 4u > (1u << 19))
     return fail(SJ_ERR_INVALID_ARGUMENT, "chunk_rows=%u", g.chunk_rows);
+  if (g.q1_cap < 2 * 32 * rpl || (g.q1_cap & (g.q1_cap - 1)) || g.q2_cap < 64 || (g.q2_cap & (g.q2_cap - 1)))
+    return fail(SJ_ERR_INVALID_ARGUMENT, "queue capacities");
   if (g.reorder_period < 2 * g.stages) g.reorder_period = 2 * g.stages;
   g.smem_bytes = probe_smem_bytes(g);
   if (g.smem_bytes > eng->smem_optin)

@@ -123,13 +123,27 @@ __host__ __device__ __forceinline__ uint32_t slot_of(int32_t k, int32_t kmin, ui
 __host__ __device__ __forceinline__ uint32_t bf_word(uint32_t slot, uint32_t log2w) {
   return log2w ? ((slot * 0x9E3779B1u) >> (32 - log2w)) : 0u;
 }
+__host__ __device__ __forceinline__ uint32_t bf_pos(uint32_t g, uint32_t j) {
+  return (g >> (26 - 6 * j)) & 63u;  // j-th 6-bit field from the top of g
+}
 __host__ __device__ __forceinline__ uint64_t bf_mask(uint32_t slot, uint32_t k) {
   const uint32_t g = slot * 0x85EBCA77u;
-  uint64_t m = 1ull << (g >> 26);
-  if (k > 1) m |= 1ull << ((g >> 20) & 63u);
-  if (k > 2) m |= 1ull << ((g >> 14) & 63u);
-  if (k > 3) m |= 1ull << ((g >> 8) & 63u);
+  uint64_t m = 0;
+  for (uint32_t j = 0; j < k; ++j) m |= 1ull << bf_pos(g, j);
   return m;
+}
+// Test of the same k bits on a 64-bit word held as two 32-bit halves (no 64-bit
+// shifts on the hot path).
+template <int K>
+__host__ __device__ __forceinline__ uint32_t bf_test_word(uint32_t lo, uint32_t hi, uint32_t slot) {
+  const uint32_t g = slot * 0x85EBCA77u;
+  uint32_t r = ~0u;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const uint32_t p = bf_pos(g, (uint32_t)j);
+    r &= ((p & 32u) ? hi : lo) >> (p & 31u);
+  }
+  return r & 1u;
 }
 
 __host__ __device__ __forceinline__ uint32_t ceil_log2(uint64_t x) {

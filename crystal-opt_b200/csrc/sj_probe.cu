@@ -1,46 +1,46 @@
 // sj_probe.cu -- the fused star-join probe: fact scan -> LIP Bloom filters -> PHT
-// probes -> group-by SUM, one persistent kernel per query.
+// probes -> group-by SUM, one persistent warp-specialized kernel per query.
 //
 // Replaces the reference's probe<128,4> kernels (src/ssb-jo/q33/0-lip.cu:28-112,
 // src/ssb-jo/q33/0-naive.cu:28-91, src/ssb-jo/q41/0-lip.cu:28-131).  Same answer,
 // different machine mapping:
-//   * Persistent grid (a multiple of the SM count).  Each CTA walks fact chunks
-//     round-robin.  Only the column tested first is read densely: its chunk is
-//     streamed by a CTA-local TMA bulk copy (cp.async.bulk, no multicast) into a
-//     ring of shared-memory stages, each completing on its own mbarrier.
-//   * Filters are evaluated on the PHT slot of each key; the filters that fit the
-//     budget are copied into shared memory once per CTA.
-//   * Survivors of the first test are compacted (warp ballot + popc, one shared
-//     atomic per warp) into ring queue Q1 with their row and slot.  Later columns
-//     are read only at survivor rows (sector-sparse reads, prefetched into L2 at
-//     enqueue time).  Survivors of the second test are compacted again into Q2;
-//     the remaining tests, the PHT probes and the aggregate run densely on Q2.
-//     Queue tails are monotonic counters read back after the sub-block barrier,
-//     so every thread holds the same head/tail values in registers and queue
-//     decisions need no extra barrier.
+//   * Persistent grid of one CTA per SM: one producer warp and NWC consumer warps.
+//     Only the column tested first is read densely.  The producer streams each
+//     chunk of it with one CTA-local TMA bulk copy (cp.async.bulk, no multicast)
+//     into a ring of shared-memory stages; "full" mbarriers signal the consumers,
+//     "empty" mbarriers (one arrival per consumer warp) give the stage back.
+//     There is no block-wide barrier in the steady state.
+//   * Each consumer warp tests its slice of the stage against the first filter
+//     (held in shared memory) and compacts the survivors (warp ballot + popc) into
+//     its own ring queue Q1 of row offsets.  Later columns are read only at
+//     survivor rows (sector-sparse reads, prefetched into L2 at enqueue time).
+//     Survivors of the second test are compacted again into the warp's Q2; the
+//     remaining tests, the PHT probes and the aggregate run densely on Q2.  Queue
+//     heads/tails are warp-uniform registers.  Values of earlier steps are not
+//     carried in the queues: the rare survivors recompute them from L2.
+//   * Filters are evaluated on the PHT slot of each key, so a filter never rejects
+//     a row the PHT would accept; filters that fit the budget live in shared memory.
 //   * Group partials (dense dictionary codes) live in shared memory and are
 //     flushed once per CTA with 64-bit atomics; group spaces that do not fit
 //     aggregate straight into global memory.
-//   * Adaptive LIP: each CTA counts probes/passes per filter and re-ranks the
-//     filter order every few chunks.  A new order applies to chunks issued after
-//     the decision; queues are drained before the first chunk of the new order is
-//     consumed, so the result never depends on the order, only the work does.
+//   * Adaptive LIP: consumer warps count probes/passes per filter; every few chunks
+//     the producer re-ranks the filter order for the chunks it issues next.  A warp
+//     drains its queues before the first chunk of a new order, so the result never
+//     depends on the order, only the work does.
 #include "sj_internal.h"
 #include "sj_ptx.cuh"
 
 namespace sj {
 
 enum : uint32_t { kStepBF = 0, kStepPHT = 1 };
+enum : int { kModeDirectSmem = 0, kModeBlockedSmem = 1, kModeBfAny = 2, kModePht = 3 };
 
 struct SmemLayout {
-  uint32_t stage_off, bar_off, bf_off, q1_row_off, q1_val_off, q2_row_off, q2_v0_off, q2_v1_off, gsum_off,
-      gcnt_off, ctl_off, total;
+  uint32_t stage_off, full_off, empty_off, bf_off, q1_off, q2_off, gsum_off, gcnt_off, ctl_off, total;
 };
 
 struct Ctl {
-  uint32_t cnt1[2], cnt2[2];      // monotonic append counters (double-buffered)
   uint32_t abort;
-  uint32_t issue_ver;
   uint32_t n_steps[2];
   uint32_t steps[2][kMaxSteps];  // (dim | kind << 4)
   uint32_t order[2][kMaxDims];
@@ -59,27 +59,24 @@ struct Ctl {
 __host__ __device__ inline uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 
 __host__ __device__ inline SmemLayout probe_layout(const SjProbeGeom& g) {
+  const uint32_t nwc = g.threads / 32 - 1;
   SmemLayout L;
   uint32_t o = 0;
   L.stage_off = o;
   o += g.stages * g.chunk_rows * 4u;
   o = align_up(o, 16);
-  L.bar_off = o;
+  L.full_off = o;
+  o += g.stages * 8u;
+  L.empty_off = o;
   o += g.stages * 8u;
   o = align_up(o, 16);
   L.bf_off = o;
   o += g.bf_smem_bytes;
   o = align_up(o, 16);
-  L.q1_row_off = o;
-  o += g.q1_cap * 4u;
-  L.q1_val_off = o;
-  o += g.q1_cap * 4u;
-  L.q2_row_off = o;
-  o += g.q2_cap * 4u;
-  L.q2_v0_off = o;
-  o += g.q2_cap * 4u;
-  L.q2_v1_off = o;
-  o += g.q2_cap * 4u;
+  L.q1_off = o;
+  o += nwc * g.q1_cap * 4u;
+  L.q2_off = o;
+  o += nwc * g.q2_cap * 4u;
   o = align_up(o, 16);
   L.gsum_off = o;
   o += g.group_smem_cap * 8u;
@@ -102,8 +99,26 @@ __device__ __forceinline__ uint64_t lds_u64(uint32_t saddr) {
   asm volatile("ld.shared.u64 %0, [%1];" : "=l"(v) : "r"(saddr));
   return v;
 }
+__device__ __forceinline__ uint2 lds_u32x2(uint32_t saddr) {
+  uint2 v;
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(saddr));
+  return v;
+}
+__device__ __forceinline__ int4 lds_v4(uint32_t saddr) {
+  int4 v;
+  asm volatile("ld.shared.v4.s32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(saddr));
+  return v;
+}
 __device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t* p) {
   return *reinterpret_cast<const volatile uint32_t*>(p);
+}
+
+// Slot of a fact key with the common in-range case first; the remainder path
+// (keys outside [key_min, key_min + len)) is a rarely taken branch.
+__device__ __forceinline__ uint32_t slot_fast(int32_t k, int32_t kmin, uint32_t len, uint64_t m) {
+  const uint32_t d = (uint32_t)k - (uint32_t)kmin;
+  if (__builtin_expect(d < len, 1)) return d;
+  return (uint32_t)__umul64hi(m * (uint64_t)d, (uint64_t)len);
 }
 
 // Per-dimension filter view held in registers.
@@ -155,35 +170,69 @@ __device__ inline float order_cost(const float* rate, const uint32_t* order, uin
   return c;
 }
 
-struct Probe {
+// Four per-dimension values held in registers, selected by a runtime dimension
+// index without local memory.
+struct Vals4 {
+  uint32_t v0, v1, v2, v3;
+  __device__ __forceinline__ uint32_t get(uint32_t d) const {
+    return d == 0 ? v0 : (d == 1 ? v1 : (d == 2 ? v2 : v3));
+  }
+  __device__ __forceinline__ void set(uint32_t d, uint32_t x) {
+    v0 = d == 0 ? x : v0;
+    v1 = d == 1 ? x : v1;
+    v2 = d == 2 ? x : v2;
+    v3 = d == 3 ? x : v3;
+  }
+};
+
+// The streamed dimension's parameters, in registers for one chunk.
+struct First {
+  const int32_t* fk;
+  const int2* ht;
+  int32_t kmin;
+  uint32_t len;
+  uint64_t fm;
+  BfView bf;
+};
+
+// State of one consumer warp.  Every field is identical in all 32 lanes.
+struct Warp {
   const SjPlanRt& P;
-  const SjProbeGeom& G;
   Ctl& c;
-  uint32_t* q1_row;
-  int32_t* q1_val;
-  uint32_t* q2_row;
-  int32_t* q2_v0;
-  int32_t* q2_v1;
+  uint32_t* q1;
+  uint32_t* q2;
+  uint32_t q1m, q2m;
   unsigned long long* s_sum;
   uint32_t* s_cnt;
-  BfView bf[kMaxDims];
-  uint64_t base_row;  // row of queue offset 0 (row_begin rounded down to 4)
+  uint32_t bf_base;
+  uint64_t base_row;
   uint64_t pol_first, pol_keep;
-  // queue state, identical in every thread of the CTA
+  uint32_t lane;
   uint32_t t1, h1, t2, h2;
-  uint32_t seen1[2], seen2[2];
-  uint32_t b1, b2;
+
+  __device__ __forceinline__ BfView bfview(uint32_t d) const {
+    BfView f;
+    const SjDimRt& D = P.dim[d];
+    f.mode = D.bf_mode;
+    f.k = D.bf_k;
+    f.log2 = c.bf_log2[d];
+    f.gptr = D.bf;
+    const uint32_t off = c.bf_in_smem[d];
+    f.smem = off == ~0u ? 0u : bf_base + off;
+    return f;
+  }
 
   __device__ __forceinline__ uint32_t slot_at(uint32_t d, uint32_t rel) const {
     const SjDimRt& D = P.dim[d];
-    return slot_of(ld_stream(D.fact_fk + base_row + rel, pol_first), D.key_min, D.ht_len, D.fastmod_m);
+    return slot_fast(ld_stream(D.fact_fk + base_row + rel, pol_first), D.key_min, D.ht_len, D.fastmod_m);
   }
 
-  __device__ void aggregate(uint32_t rel, const uint32_t* cv) {
+  __device__ __forceinline__ void aggregate(uint32_t rel, const Vals4& cv) {
     uint32_t g = 0;
-#pragma unroll
-    for (uint32_t d = 0; d < kMaxDims; ++d)
-      if (d < P.n_dims && P.dim[d].grouped) g += cv[d] * c.group_stride[d];
+    if (0 < P.n_dims && P.dim[0].grouped) g += cv.v0 * c.group_stride[0];
+    if (1 < P.n_dims && P.dim[1].grouped) g += cv.v1 * c.group_stride[1];
+    if (2 < P.n_dims && P.dim[2].grouped) g += cv.v2 * c.group_stride[2];
+    if (3 < P.n_dims && P.dim[3].grouped) g += cv.v3 * c.group_stride[3];
     int64_t m = (int64_t)ld_stream(P.measure + base_row + rel, pol_first);
     if (P.measure_sub) m -= (int64_t)ld_stream(P.measure_sub + base_row + rel, pol_first);
     if (c.groups_in_smem) {
@@ -195,161 +244,220 @@ struct Probe {
     }
   }
 
-  // Restore what steps [0, upto) produced: a slot (filter step) or a code (PHT step).
-  __device__ __forceinline__ void load_state(uint32_t ver, uint32_t upto, int32_t v0, int32_t v1, uint32_t& have,
-                                             uint32_t* sv, uint32_t* cv) {
-    have = 0;
-#pragma unroll
-    for (uint32_t p = 0; p < 2; ++p) {
-      if (p >= upto) break;
-      const uint32_t st = c.steps[ver][p];
-      const uint32_t d = st & 15u;
-      const uint32_t v = (uint32_t)(p ? v1 : v0);
-      if ((st >> 4) == kStepBF) sv[d] = v;
-      else cv[d] = v;
-      have |= 1u << d;
-    }
-  }
-
-  // Steps [2, n) for one Q2 survivor, then the aggregate.
-  __device__ void finish_row(uint32_t ver, uint32_t rel, uint32_t have, uint32_t* sv, uint32_t* cv) {
+  // Steps [first, n) for one survivor, then the aggregate.  Slots / codes a step
+  // needs and that earlier steps did not leave in registers are recomputed.
+  __device__ __forceinline__ void finish(uint32_t ver, uint32_t first, uint32_t rel, uint32_t have, uint32_t coded,
+                                         Vals4 sv, Vals4 cv) {
     const uint32_t n = c.n_steps[ver];
-    for (uint32_t p = 2; p < n; ++p) {
+    for (uint32_t p = first; p < n; ++p) {
       const uint32_t st = c.steps[ver][p];
       const uint32_t d = st & 15u;
       atomicAdd(&c.step_in[p], 1u);
       if (!((have >> d) & 1u)) {
-        sv[d] = slot_at(d, rel);
+        sv.set(d, slot_at(d, rel));
         have |= 1u << d;
       }
       if ((st >> 4) == kStepBF) {
         atomicAdd(&c.probes[d], 1u);
-        if (!bf_test(bf[d], sv[d], pol_keep)) return;
+        if (!bf_test(bfview(d), sv.get(d), pol_keep)) return;
         atomicAdd(&c.passes[d], 1u);
       } else {
-        const int2 e = ld_slot(P.dim[d].ht + sv[d], pol_keep);
+        const int2 e = ld_slot(P.dim[d].ht + sv.get(d), pol_keep);
         if (e.x == 0) return;
-        cv[d] = (uint32_t)e.y;
+        cv.set(d, (uint32_t)e.y);
+        coded |= 1u << d;
       }
       atomicAdd(&c.step_out[p], 1u);
+    }
+    // codes of grouped dimensions whose PHT probe passed in an earlier step
+    for (uint32_t d = 0; d < P.n_dims; ++d) {
+      if (!P.dim[d].grouped || ((coded >> d) & 1u)) continue;
+      const uint32_t s = ((have >> d) & 1u) ? sv.get(d) : slot_at(d, rel);
+      cv.set(d, (uint32_t)ld_slot(P.dim[d].ht + s, pol_keep).y);
     }
     aggregate(rel, cv);
   }
 
-  // Q1 entries [h1, h1 + cnt): step 1, then aggregate (plans of <= 2 steps) or
-  // compact the survivors into Q2.  Called by every thread with the same cnt.
-  __device__ void q1_round(uint32_t ver, uint32_t cnt) {
-    const uint32_t tid = threadIdx.x, lane = tid & 31u;
+  // Q1 entries [h1, h1 + cnt): step 1, then finish (plans of <= 2 steps) or
+  // compact the survivors into Q2.
+  __device__ __forceinline__ void q1_round(uint32_t ver, uint32_t cnt) {
+    __syncwarp();
     const uint32_t n = c.n_steps[ver];
-    const uint32_t st0 = c.steps[ver][0], st1 = c.steps[ver][n > 1 ? 1 : 0];
-    const uint32_t d0 = st0 & 15u, d1 = st1 & 15u;
+    const uint32_t st1 = c.steps[ver][n > 1 ? 1 : 0];
+    const uint32_t d1 = st1 & 15u;
+    const bool bf1 = (st1 >> 4) == kStepBF;
     bool pass = false;
-    uint32_t rel = 0;
-    int32_t v0 = 0, v1 = 0;
-    if (tid < cnt) {
-      const uint32_t e = (h1 + tid) & (G.q1_cap - 1);
-      rel = q1_row[e];
-      v0 = q1_val[e];
+    uint32_t rel = 0, have = 0, coded = 0;
+    Vals4 sv{0, 0, 0, 0}, cv{0, 0, 0, 0};
+    if (lane < cnt) {
+      rel = q1[(h1 + lane) & q1m];
       if (n == 1) {
         pass = true;
       } else {
-        const uint32_t s1 = (d1 == d0 && (st0 >> 4) == kStepBF) ? (uint32_t)v0 : slot_at(d1, rel);
-        if ((st1 >> 4) == kStepBF) {
-          pass = bf_test(bf[d1], s1, pol_keep);
-          v1 = (int32_t)s1;
+        const uint32_t s1 = slot_at(d1, rel);
+        sv.set(d1, s1);
+        have = 1u << d1;
+        if (bf1) {
+          pass = bf_test(bfview(d1), s1, pol_keep);
         } else {
-          const int2 e2 = ld_slot(P.dim[d1].ht + s1, pol_keep);
-          pass = e2.x != 0;
-          v1 = e2.y;
+          const int2 e = ld_slot(P.dim[d1].ht + s1, pol_keep);
+          pass = e.x != 0;
+          cv.set(d1, (uint32_t)e.y);
+          coded = 1u << d1;
         }
       }
     }
-    const uint32_t mo = __ballot_sync(0xffffffffu, pass);
+    const uint32_t m = __ballot_sync(0xffffffffu, pass);
     if (n <= 2) {
-      if (pass) {
-        uint32_t sv[kMaxDims] = {0, 0, 0, 0}, cv[kMaxDims] = {0, 0, 0, 0}, have;
-        load_state(ver, n, v0, v1, have, sv, cv);
-        aggregate(rel, cv);
-      }
-      if (n == 2 && lane == 0 && mo) atomicAdd(&c.step_out[1], (uint32_t)__popc(mo));
+      if (pass) finish(ver, 2, rel, have, coded, sv, cv);
     } else {
-      uint32_t base = 0;
-      if (lane == 0 && mo) base = atomicAdd(&c.cnt2[b2], (uint32_t)__popc(mo));
-      base = __shfl_sync(0xffffffffu, base, 0);
       if (pass) {
-        const uint32_t e = (t2 + (base - seen2[b2]) + __popc(mo & lanemask_lt())) & (G.q2_cap - 1);
-        q2_row[e] = rel;
-        q2_v0[e] = v0;
-        q2_v1[e] = v1;
-        // the column the next step reads at this row
+        q2[(t2 + __popc(m & lanemask_lt())) & q2m] = rel;
         const uint32_t d2 = c.steps[ver][2] & 15u;
-        if (d2 != d0 && d2 != d1) prefetch_l2(P.dim[d2].fact_fk + base_row + rel);
+        if (d2 != d1) prefetch_l2(P.dim[d2].fact_fk + base_row + rel);
+      }
+      t2 += __popc(m);
+    }
+    if (lane == 0 && n > 1) {
+      atomicAdd(&c.step_in[1], cnt);
+      atomicAdd(&c.step_out[1], (uint32_t)__popc(m));
+      if (bf1) {
+        atomicAdd(&c.probes[d1], cnt);
+        atomicAdd(&c.passes[d1], (uint32_t)__popc(m));
       }
     }
-    __syncthreads();
-    if (n > 2) {
-      const uint32_t cur = ld_volatile_u32(&c.cnt2[b2]);
-      const uint32_t added = cur - seen2[b2];
-      t2 += added;
-      seen2[b2] = cur;
-      b2 ^= 1u;
-      if (tid == 0) c.step_out[1] += added;
-    }
-    if (tid == 0 && n > 1) {
-      c.step_in[1] += cnt;
-      if ((st1 >> 4) == kStepBF) c.probes[d1] += cnt;
-    }
-    if (n > 1 && (st1 >> 4) == kStepBF && lane == 0 && mo) atomicAdd(&c.passes[d1], (uint32_t)__popc(mo));
     h1 += cnt;
   }
 
-  __device__ void q2_round(uint32_t ver, uint32_t cnt) {
-    const uint32_t tid = threadIdx.x;
-    if (tid < cnt) {
-      const uint32_t e = (h2 + tid) & (G.q2_cap - 1);
-      uint32_t sv[kMaxDims] = {0, 0, 0, 0}, cv[kMaxDims] = {0, 0, 0, 0}, have;
-      load_state(ver, 2, q2_v0[e], q2_v1[e], have, sv, cv);
-      finish_row(ver, q2_row[e], have, sv, cv);
-    }
-    __syncthreads();
+  __device__ __forceinline__ void q2_round(uint32_t ver, uint32_t cnt) {
+    __syncwarp();
+    if (lane < cnt) finish(ver, 2, q2[(h2 + lane) & q2m], 0u, 0u, Vals4{0, 0, 0, 0}, Vals4{0, 0, 0, 0});
     h2 += cnt;
   }
 
-  // Run queue rounds: full rounds only while streaming, everything when draining.
-  __device__ void pump(uint32_t ver, bool drain) {
-    const uint32_t nt = blockDim.x;
+  // Queue rounds: full rounds only while streaming, everything when draining.
+  __device__ __forceinline__ void pump(uint32_t ver, bool drain) {
     for (;;) {
       const uint32_t a1 = t1 - h1, a2 = t2 - h2;
-      if (a2 >= nt || (drain && a2 > 0 && a1 == 0)) {
-        q2_round(ver, min(a2, nt));
-      } else if (a1 >= nt || (drain && a1 > 0)) {
-        q1_round(ver, min(a1, nt));
+      if (a2 >= 32 || (drain && a2 > 0 && a1 == 0)) {
+        q2_round(ver, min(a2, 32u));
+      } else if (a1 >= 32 || (drain && a1 > 0)) {
+        q1_round(ver, min(a1, 32u));
       } else {
         break;
       }
     }
   }
+
+  // Test the rows [off, off + rows) of a staged chunk against the first step and
+  // queue the survivors.  FULL: every row of the chunk is valid and staged.
+  // Per lane and pass: RPL independent rows; the pass bits collect in a register
+  // mask, and one warp prefix scan of the mask popcounts places the survivors.
+  template <int RPL, int MODE, int K, bool FULL>
+  __device__ __forceinline__ uint32_t scan(uint32_t ver, uint32_t sbuf, const First& f, uint32_t off, uint32_t rows,
+                                           uint64_t cstart, uint32_t crows, uint32_t tma_rows, uint32_t skip,
+                                           uint32_t rel0, const int32_t* pf) {
+    static_assert(RPL <= 32, "pass mask is 32 bits");
+    const uint32_t t_begin = t1;
+    for (uint32_t i0 = off; i0 < off + rows; i0 += 32u * RPL) {
+      uint32_t d[RPL];
+      uint32_t valid = ~0u;  // bit j: row j of this lane lies in the scanned range
+      bool oor = false;      // some key outside [key_min, key_min + len)
+#pragma unroll
+      for (uint32_t j4 = 0; j4 < RPL / 4; ++j4) {
+        const uint32_t r4 = i0 + (j4 * 32u + lane) * 4u;
+        const int4 v = lds_v4(sbuf + r4 * 4u);
+        int32_t fk[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) {
+          if (!FULL) {
+            const uint32_t r = r4 + j;
+            const bool ok = (r < crows) && (r >= skip);
+            if (!ok) valid &= ~(1u << (j4 * 4 + j));
+            if (ok && r >= tma_rows) fk[j] = ld_stream(f.fk + cstart + r, pol_first);
+          }
+          d[j4 * 4 + j] = (uint32_t)fk[j] - (uint32_t)f.kmin;
+          oor |= d[j4 * 4 + j] >= f.len;
+        }
+      }
+      if (__any_sync(0xffffffffu, oor)) {  // rare: reduce out-of-range keys modulo len
+#pragma unroll
+        for (uint32_t j = 0; j < RPL; ++j)
+          if (d[j] >= f.len) d[j] = (uint32_t)__umul64hi(f.fm * (uint64_t)d[j], (uint64_t)f.len);
+      }
+      uint32_t mask = 0;
+#pragma unroll
+      for (uint32_t j = 0; j < RPL; ++j) {
+        const uint32_t sl = d[j];
+        bool ok;
+        if (MODE == kModeDirectSmem) {
+          ok = (lds_u32(f.bf.smem + (sl >> 5) * 4u) >> (sl & 31u)) & 1u;
+        } else if (MODE == kModeBlockedSmem) {
+          const uint2 wv = lds_u32x2(f.bf.smem + bf_word(sl, f.bf.log2) * 8u);
+          ok = bf_test_word<K>(wv.x, wv.y, sl);
+        } else if (MODE == kModeBfAny) {
+          ok = bf_test(f.bf, sl, pol_keep);
+        } else {
+          ok = ld_slot(f.ht + sl, pol_keep).x != 0;
+        }
+        mask |= (ok ? 1u : 0u) << j;
+      }
+      if (!FULL) mask &= valid;
+      const uint32_t lanes = __ballot_sync(0xffffffffu, mask != 0);
+      if (lanes) {
+        uint32_t pos, total;
+        if (__any_sync(0xffffffffu, mask & (mask - 1u))) {
+          // some lane has several survivors: warp prefix scan of the counts
+          const uint32_t cnt = __popc(mask);
+          uint32_t incl = cnt;
+#pragma unroll
+          for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+          }
+          total = __shfl_sync(0xffffffffu, incl, 31);
+          pos = t1 + incl - cnt;
+        } else {
+          // at most one survivor per lane: the lane ballot is the prefix
+          total = __popc(lanes);
+          pos = t1 + __popc(lanes & lanemask_lt());
+        }
+        while (mask) {
+          const uint32_t j = __ffs(mask) - 1u;
+          mask &= mask - 1u;
+          const uint32_t rr = rel0 + i0 + ((j >> 2) * 32u + lane) * 4u + (j & 3u);
+          q1[pos++ & q1m] = rr;
+          if (pf) prefetch_l2(pf + rr);
+        }
+        t1 += total;
+        if (t1 - h1 > q1m + 1 - 32u * RPL) pump(ver, false);  // keep room for one more pass
+      }
+    }
+    return t1 - t_begin;
+  }
 };
 
-// NT threads per CTA; RPT fact rows per thread per sub-block (multiple of 4).
-template <int NT, int RPT>
-__global__ void __launch_bounds__(NT, 1) sj_probe_kernel(const __grid_constant__ SjPlanRt P,
-                                                         const __grid_constant__ SjProbeGeom G) {
-  static_assert(RPT % 4 == 0, "rows per thread must be a multiple of 4");
-  constexpr uint32_t SB = NT * RPT;  // rows per sub-block
+// NWC consumer warps + 1 producer warp; RPL fact rows per lane per scan pass.
+template <int NWC, int RPL>
+__global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __grid_constant__ SjPlanRt P,
+                                                                     const __grid_constant__ SjProbeGeom G) {
+  static_assert(RPL % 4 == 0, "rows per lane must be a multiple of 4");
+  constexpr uint32_t NT = (NWC + 1) * 32;
   extern __shared__ __align__(128) uint8_t smem[];
   const SmemLayout L = probe_layout(G);
   int32_t* stage = reinterpret_cast<int32_t*>(smem + L.stage_off);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
+  uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
   uint8_t* bfmem = smem + L.bf_off;
   Ctl& c = *reinterpret_cast<Ctl*>(smem + L.ctl_off);
   const SjDesc* desc = P.desc;
-  const uint32_t tid = threadIdx.x, lane = tid & 31u;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const uint32_t S = G.stages, CH = G.chunk_rows;
 
   const uint64_t base_row = P.row_begin & ~3ull;
   const uint64_t span = P.row_end - base_row;
   const uint32_t n_chunks = (uint32_t)((span + CH - 1) / CH);
+  const uint32_t my_iters = (blockIdx.x < n_chunks) ? (n_chunks - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
 
   // ---- setup (thread 0): plan steps, filter placement, mbarriers ----------
   if (tid == 0) {
@@ -374,12 +482,15 @@ __global__ void __launch_bounds__(NT, 1) sj_probe_kernel(const __grid_constant__
     for (uint32_t d = 0; d < P.n_dims; ++d) c.group_stride[d] = desc->dim[d].group_stride;
     c.n_groups = desc->n_groups;
     c.groups_in_smem = c.n_groups <= G.group_smem_cap;
-    for (uint32_t s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+    for (uint32_t s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NWC);
+    }
     mbar_fence_init();
   }
   __syncthreads();
 
-  // ---- copy filters into shared memory, zero group partials ---------------
+  // ---- filters into shared memory, zero the group partials ----------------
   for (uint32_t d = 0; d < P.n_dims; ++d) {
     if (c.bf_in_smem[d] == ~0u) continue;
     const SjDimRt& D = P.dim[d];
@@ -392,213 +503,174 @@ __global__ void __launch_bounds__(NT, 1) sj_probe_kernel(const __grid_constant__
       *reinterpret_cast<uint2*>(bfmem + c.bf_in_smem[d]) = *reinterpret_cast<const uint2*>(D.bf);
     }
   }
-  Probe pr{P, G, c,
-           reinterpret_cast<uint32_t*>(smem + L.q1_row_off),
-           reinterpret_cast<int32_t*>(smem + L.q1_val_off),
-           reinterpret_cast<uint32_t*>(smem + L.q2_row_off),
-           reinterpret_cast<int32_t*>(smem + L.q2_v0_off),
-           reinterpret_cast<int32_t*>(smem + L.q2_v1_off),
-           reinterpret_cast<unsigned long long*>(smem + L.gsum_off),
-           reinterpret_cast<uint32_t*>(smem + L.gcnt_off)};
+  unsigned long long* s_sum = reinterpret_cast<unsigned long long*>(smem + L.gsum_off);
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + L.gcnt_off);
   if (c.groups_in_smem) {
     for (uint32_t g = tid; g < c.n_groups; g += NT) {
-      pr.s_sum[g] = 0ull;
-      pr.s_cnt[g] = 0u;
+      s_sum[g] = 0ull;
+      s_cnt[g] = 0u;
     }
   }
-#pragma unroll
-  for (uint32_t d = 0; d < kMaxDims; ++d) {
-    pr.bf[d].mode = kBfDirect;
-    pr.bf[d].k = 1;
-    pr.bf[d].log2 = 0;
-    pr.bf[d].gptr = nullptr;
-    pr.bf[d].smem = 0;
-    if (d < P.n_dims) {
-      const SjDimRt& D = P.dim[d];
-      pr.bf[d].mode = D.bf_mode;
-      pr.bf[d].k = D.bf_k;
-      pr.bf[d].log2 = c.bf_log2[d];
-      pr.bf[d].gptr = D.bf;
-      pr.bf[d].smem = (c.bf_in_smem[d] == ~0u) ? 0u : smem_addr(bfmem + c.bf_in_smem[d]);
-    }
-  }
-  pr.base_row = base_row;
-  pr.pol_first = policy_evict_first();
-  pr.pol_keep = policy_evict_last();
-  pr.t1 = pr.h1 = pr.t2 = pr.h2 = 0;
-  pr.seen1[0] = pr.seen1[1] = pr.seen2[0] = pr.seen2[1] = 0;
-  pr.b1 = pr.b2 = 0;
   __syncthreads();
 
-  // ---- TMA producer (thread 0) --------------------------------------------
-  const uint32_t my_iters = (blockIdx.x < n_chunks) ? (n_chunks - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
-  uint32_t issued = 0;  // meaningful in thread 0
-  auto issue = [&](uint32_t it) {
-    const uint32_t s = it % S;
-    const uint32_t chunk = blockIdx.x + it * gridDim.x;
-    const uint32_t ver = c.issue_ver;
-    const uint32_t d = c.order[ver][0];
-    c.stage_ver[s] = ver;
-    const uint64_t start = base_row + (uint64_t)chunk * CH;
-    const uint64_t rows = min((uint64_t)CH, P.row_end - start);
-    const uint32_t bytes = (uint32_t)(rows & ~3ull) * 4u;
-    fence_proxy_async_smem();
-    if (bytes) {
-      mbar_arrive_expect_tx(&bar[s], bytes);
-      bulk_g2s(stage + (size_t)s * CH, P.dim[d].fact_fk + start, bytes, &bar[s], pr.pol_first);
-    } else {
-      mbar_arrive(&bar[s]);
-    }
-  };
-  if (tid == 0) {
-    for (; issued < S && issued < my_iters; ++issued) issue(issued);
-  }
+  const uint64_t pol_first = policy_evict_first();
+  const uint64_t pol_keep = policy_evict_last();
 
-  // ---- main loop -----------------------------------------------------------
-  uint32_t exec_ver = 0;
-  uint32_t it = 0;
-  for (; it < my_iters; ++it) {
-    const uint32_t s = it % S;
-    const uint32_t chunk = blockIdx.x + it * gridDim.x;
-    if (!mbar_wait_bounded(&bar[s], (it / S) & 1u, kMaxPolls)) c.abort = 1;
-    __syncthreads();
-    if (c.abort) break;
-    const uint32_t sver = c.stage_ver[s];
-    if (sver != exec_ver) {
-      // first chunk of a new filter order: drain the queues under the old one
-      pr.pump(exec_ver, true);
-      exec_ver = sver;
-    }
-    const uint32_t ver = exec_ver;
-    const uint32_t st0 = c.steps[ver][0];
-    const uint32_t d0 = st0 & 15u;
-    const SjDimRt& D0 = P.dim[d0];
-    const BfView f0 = pr.bf[d0];
-    const bool is_bf = (st0 >> 4) == kStepBF;
-    const uint64_t cstart = base_row + (uint64_t)chunk * CH;
-    const uint32_t crows = (uint32_t)min((uint64_t)CH, P.row_end - cstart);
-    const uint32_t tma_rows = crows & ~3u;
-    const uint32_t skip = (cstart < P.row_begin) ? (uint32_t)(P.row_begin - cstart) : 0u;
-    const uint32_t rel0 = (uint32_t)(cstart - base_row);
-    const int32_t* pf = nullptr;  // column read at survivor rows by step 1
-    if (c.n_steps[ver] > 1) {
-      const uint32_t d1 = c.steps[ver][1] & 15u;
-      if (d1 != d0) pf = P.dim[d1].fact_fk + base_row;
-    }
-    const int32_t* sbuf = stage + (size_t)s * CH;
-    const uint32_t t1_before = pr.t1;
-
-    for (uint32_t sb = 0; sb < CH; sb += SB) {
-      bool pass[RPT];
-      int32_t val[RPT];
-#pragma unroll
-      for (uint32_t k = 0; k < RPT / 4; ++k) {
-        const uint32_t r4 = sb + (k * NT + tid) * 4u;  // first row of this int4
-        int4 v = *reinterpret_cast<const int4*>(sbuf + r4);
-        int32_t fk[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (uint32_t j = 0; j < 4; ++j) {
-          const uint32_t r = r4 + j;
-          const bool valid = (r < crows) && (r >= skip);
-          if (valid && r >= tma_rows) fk[j] = ld_stream(D0.fact_fk + cstart + r, pr.pol_first);
-          const uint32_t sl = slot_of(fk[j], D0.key_min, D0.ht_len, D0.fastmod_m);
-          bool ok;
-          int32_t vv;
-          if (is_bf) {
-            ok = valid && bf_test(f0, sl, pr.pol_keep);
-            vv = (int32_t)sl;
-          } else {
-            int2 e = valid ? ld_slot(D0.ht + sl, pr.pol_keep) : make_int2(0, 0);
-            ok = e.x != 0;
-            vv = e.y;
+  if (warp == NWC) {
+    // ---- producer: one lane issues every chunk's TMA copy -------------------
+    if (lane == 0) {
+      uint32_t issue_ver = 0, last_switch = 0, it = 0;
+      bool aborted = false;
+      for (; it < my_iters; ++it) {
+        const uint32_t s = it % S;
+        if (it >= S && !mbar_wait_bounded(&empty[s], ((it / S) - 1u) & 1u, kMaxPolls)) {
+          aborted = true;
+          break;
+        }
+        if (ld_volatile_u32(&c.abort)) {
+          aborted = true;
+          break;
+        }
+        // adaptive re-ranking of the filter order for the chunks issued from here on
+        if (P.lip && P.adaptive && P.n_dims > 1 && it >= last_switch + 2 * S &&
+            (it == 2 * S || it % G.reorder_period == 0)) {
+          float rate[kMaxDims];
+          for (uint32_t d = 0; d < kMaxDims; ++d) {
+            const float pr = (float)ld_volatile_u32(&c.probes[d]);
+            const float pa = (float)ld_volatile_u32(&c.passes[d]);
+            rate[d] = (d < P.n_dims) ? (pa + 1.f) / (pr + 2.f) : 1.f;
           }
-          pass[k * 4 + j] = ok;
-          val[k * 4 + j] = vv;
-        }
-      }
-      uint32_t m[RPT], tot = 0;
-#pragma unroll
-      for (uint32_t j = 0; j < RPT; ++j) {
-        m[j] = __ballot_sync(0xffffffffu, pass[j]);
-        tot += __popc(m[j]);
-      }
-      uint32_t base = 0;
-      if (lane == 0 && tot) base = atomicAdd(&c.cnt1[pr.b1], tot);
-      base = __shfl_sync(0xffffffffu, base, 0);
-      uint32_t pos = pr.t1 + (base - pr.seen1[pr.b1]);
-      const uint32_t lt = lanemask_lt();
-#pragma unroll
-      for (uint32_t j = 0; j < RPT; ++j) {
-        if (pass[j]) {
-          const uint32_t rrow = rel0 + sb + ((j / 4) * NT + tid) * 4u + (j & 3u);
-          const uint32_t e = (pos + __popc(m[j] & lt)) & (G.q1_cap - 1);
-          pr.q1_row[e] = rrow;
-          pr.q1_val[e] = val[j];
-          if (pf) prefetch_l2(pf + rrow);
-        }
-        pos += __popc(m[j]);
-      }
-      __syncthreads();  // entries visible; counter final for this sub-block
-      const uint32_t cur = ld_volatile_u32(&c.cnt1[pr.b1]);
-      pr.t1 += cur - pr.seen1[pr.b1];
-      pr.seen1[pr.b1] = cur;
-      pr.b1 ^= 1u;
-      pr.pump(ver, false);
-    }
-    // The stage has been read by every thread (barrier in the last sub-block).
-    if (tid == 0) {
-      const uint32_t valid_rows = crows - skip;
-      const uint32_t passed = pr.t1 - t1_before;
-      c.rows_scanned += valid_rows;
-      c.step_in[0] += valid_rows;
-      c.step_out[0] += passed;
-      if (is_bf) {
-        c.probes[d0] += valid_rows;
-        c.passes[d0] += passed;
-      }
-      // adaptive re-ranking of the filter order
-      if (P.lip && P.adaptive && P.n_dims > 1 && exec_ver == c.issue_ver && ((it + 1) % G.reorder_period) == 0) {
-        float rate[kMaxDims];
-        for (uint32_t d = 0; d < kMaxDims; ++d)
-          rate[d] = (d < P.n_dims) ? ((float)c.passes[d] + 1.f) / ((float)c.probes[d] + 2.f) : 1.f;
-        uint32_t cand[kMaxDims];
-        const uint32_t* cur = c.order[c.issue_ver];
-        for (uint32_t d = 0; d < P.n_dims; ++d) cand[d] = cur[d];
-        for (uint32_t a = 1; a < P.n_dims; ++a)  // insertion sort by rate
-          for (uint32_t b = a; b > 0 && rate[cand[b]] < rate[cand[b - 1]]; --b) {
-            const uint32_t t = cand[b];
-            cand[b] = cand[b - 1];
-            cand[b - 1] = t;
+          uint32_t cand[kMaxDims];
+          const uint32_t* cur = c.order[issue_ver];
+          for (uint32_t d = 0; d < P.n_dims; ++d) cand[d] = cur[d];
+          for (uint32_t a = 1; a < P.n_dims; ++a)  // insertion sort by rate
+            for (uint32_t b = a; b > 0 && rate[cand[b]] < rate[cand[b - 1]]; --b) {
+              const uint32_t t = cand[b];
+              cand[b] = cand[b - 1];
+              cand[b - 1] = t;
+            }
+          if (order_cost(rate, cand, P.n_dims) < 0.9f * order_cost(rate, cur, P.n_dims)) {
+            const uint32_t nv = issue_ver ^ 1u;
+            for (uint32_t d = 0; d < kMaxDims; ++d) c.order[nv][d] = (d < P.n_dims) ? cand[d] : 0u;
+            c.n_steps[nv] = make_steps(P, c.order[nv], c.steps[nv]);
+            issue_ver = nv;
+            last_switch = it;
+            c.reorders++;
           }
-        if (order_cost(rate, cand, P.n_dims) < 0.9f * order_cost(rate, cur, P.n_dims)) {
-          const uint32_t nv = c.issue_ver ^ 1u;
-          for (uint32_t d = 0; d < kMaxDims; ++d) c.order[nv][d] = (d < P.n_dims) ? cand[d] : 0u;
-          c.n_steps[nv] = make_steps(P, c.order[nv], c.steps[nv]);
-          c.issue_ver = nv;
-          c.reorders++;
+        }
+        const uint32_t chunk = blockIdx.x + it * gridDim.x;
+        const uint32_t d = c.order[issue_ver][0];
+        c.stage_ver[s] = issue_ver;
+        const uint64_t start = base_row + (uint64_t)chunk * CH;
+        const uint64_t rows = min((uint64_t)CH, P.row_end - start);
+        const uint32_t bytes = (uint32_t)(rows & ~3ull) * 4u;
+        fence_proxy_async_smem();
+        if (bytes) {
+          mbar_arrive_expect_tx(&full[s], bytes);
+          bulk_g2s(stage + (size_t)s * CH, P.dim[d].fact_fk + start, bytes, &full[s], pol_first);
+        } else {
+          mbar_arrive(&full[s]);
         }
       }
-      if (issued < my_iters) {
-        issue(issued);
-        ++issued;
+      if (aborted) {
+        c.abort = 1;
+        // let copies still in flight land before the CTA's shared memory goes away
+        const uint32_t lo = it > S ? it - S : 0u;
+        for (uint32_t j = lo; j < it; ++j) mbar_wait_bounded(&full[j % S], (j / S) & 1u, kMaxPolls);
       }
     }
-  }
-  const bool aborted = c.abort != 0;
-  if (!aborted) {
-    pr.pump(exec_ver, true);
-  } else if (tid == 0) {
-    // let copies still in flight land before the CTA's shared memory goes away
-    for (uint32_t j = it; j < issued; ++j) mbar_wait_bounded(&bar[j % S], (j / S) & 1u, kMaxPolls);
+  } else {
+    // ---- consumer warps ------------------------------------------------------
+    Warp w{P, c,
+           reinterpret_cast<uint32_t*>(smem + L.q1_off) + warp * G.q1_cap,
+           reinterpret_cast<uint32_t*>(smem + L.q2_off) + warp * G.q2_cap,
+           G.q1_cap - 1, G.q2_cap - 1, s_sum, s_cnt, smem_addr(bfmem), base_row, pol_first, pol_keep, lane,
+           0, 0, 0, 0};
+    const uint32_t slice = CH / NWC;
+    const uint32_t my_off = warp * slice;
+    uint32_t exec_ver = 0;
+    bool aborted = false;
+    for (uint32_t it = 0; it < my_iters; ++it) {
+      const uint32_t s = it % S;
+      if (!mbar_wait_bounded(&full[s], (it / S) & 1u, kMaxPolls)) {
+        c.abort = 1;
+        aborted = true;
+        break;
+      }
+      if (ld_volatile_u32(&c.abort)) {
+        aborted = true;
+        break;
+      }
+      const uint32_t sver = c.stage_ver[s];
+      if (sver != exec_ver) {
+        w.pump(exec_ver, true);  // first chunk of a new filter order
+        exec_ver = sver;
+      }
+      const uint32_t ver = exec_ver;
+      const uint32_t st0 = c.steps[ver][0];
+      const uint32_t d0 = st0 & 15u;
+      First f;
+      f.fk = P.dim[d0].fact_fk;
+      f.ht = P.dim[d0].ht;
+      f.kmin = P.dim[d0].key_min;
+      f.len = P.dim[d0].ht_len;
+      f.fm = P.dim[d0].fastmod_m;
+      f.bf = w.bfview(d0);
+      const bool is_bf = (st0 >> 4) == kStepBF;
+      const int mode = !is_bf ? kModePht
+                              : (!f.bf.smem ? kModeBfAny : (f.bf.mode == kBfDirect ? kModeDirectSmem : kModeBlockedSmem));
+      const uint32_t chunk = blockIdx.x + it * gridDim.x;
+      const uint64_t cstart = base_row + (uint64_t)chunk * CH;
+      const uint32_t crows = (uint32_t)min((uint64_t)CH, P.row_end - cstart);
+      const uint32_t tma_rows = crows & ~3u;
+      const uint32_t skip = (cstart < P.row_begin) ? (uint32_t)(P.row_begin - cstart) : 0u;
+      const uint32_t rel0 = (uint32_t)(cstart - base_row);
+      const int32_t* pf = nullptr;  // column read at survivor rows by step 1
+      if (c.n_steps[ver] > 1) {
+        const uint32_t d1 = c.steps[ver][1] & 15u;
+        if (d1 != d0) pf = P.dim[d1].fact_fk + base_row;
+      }
+      const uint32_t sbuf = smem_addr(stage + (size_t)s * CH);
+      const bool fullc = (crows == CH) && (skip == 0);
+      uint32_t passed;
+#define SJ_SCAN(M, K)                                                                                            \
+  passed = fullc ? w.scan<RPL, M, K, true>(ver, sbuf, f, my_off, slice, cstart, crows, tma_rows, skip, rel0, pf) \
+                 : w.scan<RPL, M, K, false>(ver, sbuf, f, my_off, slice, cstart, crows, tma_rows, skip, rel0, pf)
+      if (mode == kModeDirectSmem) SJ_SCAN(kModeDirectSmem, 0);
+      else if (mode == kModeBlockedSmem) {
+        if (f.bf.k == 1) SJ_SCAN(kModeBlockedSmem, 1);
+        else if (f.bf.k == 2) SJ_SCAN(kModeBlockedSmem, 2);
+        else if (f.bf.k == 3) SJ_SCAN(kModeBlockedSmem, 3);
+        else SJ_SCAN(kModeBlockedSmem, 4);
+      } else if (mode == kModeBfAny) SJ_SCAN(kModeBfAny, 0);
+      else SJ_SCAN(kModePht, 0);
+#undef SJ_SCAN
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&empty[s]);  // this warp is done reading the stage
+        const uint32_t lo = max(my_off, skip), hi = min(my_off + slice, crows);
+        const uint32_t valid = hi > lo ? hi - lo : 0u;
+        atomicAdd(&c.rows_scanned, valid);
+        atomicAdd(&c.step_in[0], valid);
+        atomicAdd(&c.step_out[0], passed);
+        if (is_bf) {
+          atomicAdd(&c.probes[d0], valid);
+          atomicAdd(&c.passes[d0], passed);
+        }
+      }
+      w.pump(ver, false);
+    }
+    if (!aborted) w.pump(exec_ver, true);
   }
   __syncthreads();
 
   // ---- flush group partials and counters -----------------------------------
+  const bool aborted = ld_volatile_u32(&c.abort) != 0;
   if (!aborted && c.groups_in_smem) {
     for (uint32_t g = tid; g < c.n_groups; g += NT) {
-      const uint32_t cnt = pr.s_cnt[g];
+      const uint32_t cnt = s_cnt[g];
       if (cnt) {
-        atomicAdd(&P.g_sum[g], pr.s_sum[g]);
+        atomicAdd(&P.g_sum[g], s_sum[g]);
         atomicAdd(&P.g_cnt[g], (unsigned long long)cnt);
       }
     }
@@ -646,27 +718,26 @@ __global__ void __launch_bounds__(256) sj_finalize_kernel(const __grid_constant_
 // ---- host-side launchers ---------------------------------------------------
 uint32_t probe_smem_bytes(const SjProbeGeom& g) { return probe_layout(g).total; }
 
-template <int NT, int RPT>
+template <int NWC, int RPL>
 static cudaError_t launch_probe_t(const SjPlanRt& P, const SjProbeGeom& G, uint32_t smem, cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(sj_probe_kernel<NT, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = cudaFuncSetAttribute(sj_probe_kernel<NWC, RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  sj_probe_kernel<NT, RPT><<<G.grid, NT, smem, st>>>(P, G);
+  sj_probe_kernel<NWC, RPL><<<G.grid, (NWC + 1) * 32, smem, st>>>(P, G);
   return cudaGetLastError();
 }
 
-// rows_per_thread: 4, 8 or 16 rows per thread per sub-block.
-cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_per_thread, cudaStream_t st) {
+// G.threads = 32 * (consumer warps + 1); rows_per_lane: rows each lane tests per pass.
+cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_per_lane, cudaStream_t st) {
   const uint32_t smem = probe_layout(G).total;
-#define SJ_CASE(N, R) \
-  if (G.threads == N && rows_per_thread == R) return launch_probe_t<N, R>(P, G, smem, st);
-  SJ_CASE(256, 4)
-  SJ_CASE(256, 8)
-  SJ_CASE(256, 16)
-  SJ_CASE(512, 4)
-  SJ_CASE(512, 8)
-  SJ_CASE(512, 16)
-  SJ_CASE(1024, 4)
-  SJ_CASE(1024, 8)
+  const uint32_t nwc = G.threads / 32 - 1;
+#define SJ_CASE(W, R) \
+  if (nwc == W && rows_per_lane == R) return launch_probe_t<W, R>(P, G, smem, st);
+  SJ_CASE(7, 8)
+  SJ_CASE(7, 16)
+  SJ_CASE(15, 8)
+  SJ_CASE(15, 16)
+  SJ_CASE(23, 4)
+  SJ_CASE(23, 8)
 #undef SJ_CASE
   return cudaErrorInvalidValue;
 }
