@@ -536,12 +536,109 @@ struct Staging {
 };
 }  // namespace
 
+// Device address of a column a kernel may read directly: device memory, managed
+// memory, or pinned host memory mapped into the device's address space.
+static bool device_readable(const void* p, const int32_t** dev) {
+  if (!p) {
+    *dev = nullptr;
+    return true;
+  }
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if ((a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) &&
+      a.devicePointer) {
+    *dev = reinterpret_cast<const int32_t*>(a.devicePointer);
+    return true;
+  }
+  return false;
+}
+
+static sj_status run_query_whole(sj_engine* eng, const sj_plan& p, sj_group_row* out, int64_t cap, int64_t* n_out,
+                                 cudaStream_t st, cudaEvent_t t1) {
+  sj_query* q = nullptr;
+  sj_status s = sj_query_prepare(eng, &p, &q);
+  if (s == SJ_OK) s = sj_query_build(q, st);
+  if (s == SJ_OK) s = sj_query_probe(q, st);
+  cudaEventRecord(t1, st);
+  if (s == SJ_OK) s = sj_query_fetch(q, out, cap, n_out, st);
+  if (q) sj_query_release(q);
+  return s;
+}
+
+// Host-column query: the dimension tables are copied to the device; the fact
+// column tested first streams to the device in pieces on a second stream,
+// overlapped with probe launches over the pieces already present (group
+// partials accumulate across launches); the other fact columns stay in pinned
+// host memory and are read in place at survivor rows only.
+static sj_status run_query_streamed(sj_engine* eng, sj_plan p, const int32_t* host_first, sj_group_row* out,
+                                    int64_t cap, int64_t* n_out, cudaStream_t st, cudaEvent_t t1) {
+  const int first = p.order[0];
+  const int64_t b = p.row_begin, e = p.row_end;
+  const int64_t base = b & ~3ll;
+  int32_t* dev = nullptr;
+  SJ_CUDA(cudaMallocFromPoolAsync((void**)&dev, std::max<size_t>(16, 4 * (size_t)p.fact_rows), eng->pool, st));
+  p.dims[first].fact_fk = dev;
+  p.adaptive = 0;  // the streamed column is fixed; the others are host-resident
+  sj_query* q = nullptr;
+  sj_status s = sj_query_prepare(eng, &p, &q);
+  cudaStream_t cs = nullptr;
+  std::vector<cudaEvent_t> evs;
+  if (s == SJ_OK) s = sj_query_build(q, st);
+  if (s == SJ_OK) {
+    cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    cudaEvent_t ready;
+    cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    cudaEventRecord(ready, st);  // the allocation is ordered on st
+    cudaStreamWaitEvent(cs, ready, 0);
+    evs.push_back(ready);
+    const int64_t span = e - base;
+    const int64_t pieces = std::max<int64_t>(1, std::min<int64_t>(8, span / (1ll << 20)));
+    int64_t pb = base;
+    for (int64_t i = 0; i < pieces && s == SJ_OK; ++i) {
+      int64_t pe = (i + 1 == pieces) ? e : ((base + span * (i + 1) / pieces) & ~3ll);
+      if (pe <= pb) continue;
+      cudaError_t ce = cudaMemcpyAsync(dev + pb, host_first + pb, 4 * (size_t)(pe - pb), cudaMemcpyHostToDevice, cs);
+      cudaEvent_t ev;
+      cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      cudaEventRecord(ev, cs);
+      evs.push_back(ev);
+      cudaStreamWaitEvent(st, ev, 0);
+      SjPlanRt rt = q->rt;
+      rt.row_begin = (uint64_t)std::max<int64_t>(pb, b);
+      rt.row_end = (uint64_t)pe;
+      if (ce == cudaSuccess) ce = launch_probe(rt, q->geom, q->rows_per_thread, st);
+      if (ce != cudaSuccess) s = fail(SJ_ERR_CUDA, "streamed probe: %s", cudaGetErrorString(ce));
+      pb = pe;
+    }
+  }
+  if (s == SJ_OK) {
+    cudaError_t ce = launch_finalize(q->rt, (uint32_t)q->group_capacity, st);
+    if (ce != cudaSuccess) s = fail(SJ_ERR_CUDA, "finalize: %s", cudaGetErrorString(ce));
+    q->built = q->probed = true;
+    q->stream = st;
+  }
+  cudaEventRecord(t1, st);
+  if (s == SJ_OK) s = sj_query_fetch(q, out, cap, n_out, st);
+  cudaStreamSynchronize(st);
+  for (cudaEvent_t ev : evs) cudaEventDestroy(ev);
+  if (cs) cudaStreamDestroy(cs);
+  if (q) sj_query_release(q);
+  cudaFreeAsync(dev, st);
+  return s;
+}
+
 extern "C" sj_status sj_run_plain(sj_engine* eng, const sj_plan* plan, int host_columns, sj_group_row* out,
                                   int64_t cap, int64_t* n_out, float* ms, void* stream) {
   if (!eng || !plan || !n_out) return fail(SJ_ERR_INVALID_ARGUMENT, "NULL engine/plan/n_out");
   cudaStream_t st = (cudaStream_t)stream;
   SJ_CUDA(cudaSetDevice(eng->device));
+  sj_status s = validate_plan(plan);
+  if (s != SJ_OK) return s;
   sj_plan p = *plan;
+  if (p.row_end < 0) p.row_end = p.fact_rows;
   Staging stg;
   stg.pool = eng->pool;
   stg.st = st;
@@ -549,40 +646,44 @@ extern "C" sj_status sj_run_plain(sj_engine* eng, const sj_plan* plan, int host_
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
   cudaEventRecord(t0, st);
-  if (host_columns) {
-    const int64_t fr = p.fact_rows;
+  if (!host_columns) {
+    s = run_query_whole(eng, p, out, cap, n_out, st, t1);
+  } else {
+    // dimension tables: small, copied
     cudaError_t e = cudaSuccess;
     for (int d = 0; d < p.n_dims && e == cudaSuccess; ++d) {
       sj_dim& D = p.dims[d];
-      e = stg.get(plan->dims[d].fact_fk, fr, &D.fact_fk);
-      if (e == cudaSuccess) e = stg.get(plan->dims[d].key, D.rows, &D.key);
+      e = stg.get(plan->dims[d].key, D.rows, &D.key);
       if (e == cudaSuccess) e = stg.get(plan->dims[d].filter_attr, D.rows, &D.filter_attr);
       if (e == cudaSuccess) e = stg.get(plan->dims[d].payload, D.rows, &D.payload);
     }
-    if (e == cudaSuccess) e = stg.get(plan->measure, fr, &p.measure);
-    if (e == cudaSuccess) e = stg.get(plan->measure_sub, fr, &p.measure_sub);
-    if (e != cudaSuccess) {
-      cudaEventDestroy(t0);
-      cudaEventDestroy(t1);
-      return fail(e == cudaErrorMemoryAllocation ? SJ_ERR_OUT_OF_MEMORY : SJ_ERR_CUDA, "staging host columns: %s",
-                  cudaGetErrorString(e));
+    // fact columns: read in place when the device can address them (pinned)
+    bool mapped = true;
+    for (int d = 0; d < p.n_dims; ++d) mapped = mapped && device_readable(plan->dims[d].fact_fk, &p.dims[d].fact_fk);
+    mapped = mapped && device_readable(plan->measure, &p.measure) &&
+             device_readable(plan->measure_sub, &p.measure_sub);
+    if (e == cudaSuccess && mapped) {
+      s = run_query_streamed(eng, p, plan->dims[p.order[0]].fact_fk, out, cap, n_out, st, t1);
+    } else if (e == cudaSuccess) {
+      // pageable host memory: stage every fact column
+      const int64_t fr = p.fact_rows;
+      for (int d = 0; d < p.n_dims && e == cudaSuccess; ++d) e = stg.get(plan->dims[d].fact_fk, fr, &p.dims[d].fact_fk);
+      if (e == cudaSuccess) e = stg.get(plan->measure, fr, &p.measure);
+      if (e == cudaSuccess) e = stg.get(plan->measure_sub, fr, &p.measure_sub);
+      if (e == cudaSuccess) s = run_query_whole(eng, p, out, cap, n_out, st, t1);
     }
+    if (e != cudaSuccess)
+      s = fail(e == cudaErrorMemoryAllocation ? SJ_ERR_OUT_OF_MEMORY : SJ_ERR_CUDA, "staging host columns: %s",
+               cudaGetErrorString(e));
   }
-  sj_query* q = nullptr;
-  sj_status s = sj_query_prepare(eng, &p, &q);
-  if (s == SJ_OK) s = sj_query_build(q, stream);
-  if (s == SJ_OK) s = sj_query_probe(q, stream);
-  cudaEventRecord(t1, st);
-  if (s == SJ_OK) s = sj_query_fetch(q, out, cap, n_out, stream);
   if (ms) {
     cudaEventSynchronize(t1);
     float v = 0.f;
-    cudaEventElapsedTime(&v, t0, t1);
-    *ms = v;
+    if (cudaEventElapsedTime(&v, t0, t1) == cudaSuccess) *ms = v;
+    cudaGetLastError();
   }
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
-  if (q) sj_query_release(q);
   return s;
 }
 

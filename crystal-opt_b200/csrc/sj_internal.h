@@ -115,35 +115,42 @@ __host__ __device__ __forceinline__ uint32_t slot_of(int32_t k, int32_t kmin, ui
 #endif
 }
 
-// Register-blocked filter geometry of PHT slot s: one 64-bit word, chosen by the
-// top bits of a Fibonacci multiplicative hash (Knuth, TAOCP vol. 3, 6.4), and a
-// mask of k bits whose positions are 6-bit fields from the top of a second,
-// independent multiplicative hash.  Keying on the slot (not the raw key) makes
-// the filter agree with the PHT: it never rejects a row whose slot is occupied.
+// Register-blocked filter geometry of PHT slot s: one 64-bit word chosen by the
+// top bits of h = s * 0x9E3779B1 (Fibonacci multiplicative hashing, Knuth TAOCP
+// vol. 3, 6.4), and k bits inside that word.  Bit j lies in the low 32-bit half
+// for even j and in the high half for odd j (a split-block layout: the probe
+// tests each bit with one 32-bit rotate), at a 5-bit position taken from the top
+// of g = (h ^ (h >> 15)) * 0x846CA68B, a multiply-xorshift-multiply mix that
+// decorrelates the positions from the word index on sequential slot numbers.
+// Keying on the slot (not the raw key) makes the filter agree with the PHT: it
+// never rejects a row whose slot is occupied.
+__host__ __device__ __forceinline__ uint32_t bf_h1(uint32_t slot) { return slot * 0x9E3779B1u; }
+__host__ __device__ __forceinline__ uint32_t bf_g(uint32_t h1) { return (h1 ^ (h1 >> 15)) * 0x846CA68Bu; }
 __host__ __device__ __forceinline__ uint32_t bf_word(uint32_t slot, uint32_t log2w) {
-  return log2w ? ((slot * 0x9E3779B1u) >> (32 - log2w)) : 0u;
+  return log2w ? (bf_h1(slot) >> (32 - log2w)) : 0u;
 }
-__host__ __device__ __forceinline__ uint32_t bf_pos(uint32_t g, uint32_t j) {
-  return (g >> (26 - 6 * j)) & 63u;  // j-th 6-bit field from the top of g
-}
+// position (0..31) of bit j within its half
+__host__ __device__ __forceinline__ uint32_t bf_pos(uint32_t g, uint32_t j) { return (g >> (27 - 5 * j)) & 31u; }
 __host__ __device__ __forceinline__ uint64_t bf_mask(uint32_t slot, uint32_t k) {
-  const uint32_t g = slot * 0x85EBCA77u;
+  const uint32_t g = bf_g(bf_h1(slot));
   uint64_t m = 0;
-  for (uint32_t j = 0; j < k; ++j) m |= 1ull << bf_pos(g, j);
+  for (uint32_t j = 0; j < k; ++j) m |= (1ull << bf_pos(g, j)) << (32 * (j & 1u));
   return m;
 }
-// Test of the same k bits on a 64-bit word held as two 32-bit halves (no 64-bit
-// shifts on the hot path).
+// Probe-side test of the same k bits on a word held as two 32-bit halves.
 template <int K>
-__host__ __device__ __forceinline__ uint32_t bf_test_word(uint32_t lo, uint32_t hi, uint32_t slot) {
-  const uint32_t g = slot * 0x85EBCA77u;
-  uint32_t r = ~0u;
-#pragma unroll
-  for (int j = 0; j < K; ++j) {
-    const uint32_t p = bf_pos(g, (uint32_t)j);
-    r &= ((p & 32u) ? hi : lo) >> (p & 31u);
-  }
+__host__ __device__ __forceinline__ uint32_t bf_test_word(uint32_t lo, uint32_t hi, uint32_t g) {
+#ifdef __CUDA_ARCH__
+  uint32_t r = __funnelshift_r(lo, lo, g >> 27);  // rotate: uses the shift modulo 32
+  if (K > 1) r &= __funnelshift_r(hi, hi, g >> 22);
+  if (K > 2) r &= __funnelshift_r(lo, lo, g >> 17);
+  if (K > 3) r &= __funnelshift_r(hi, hi, g >> 12);
   return r & 1u;
+#else
+  uint32_t r = 1u;
+  for (int j = 0; j < K; ++j) r &= (((j & 1) ? hi : lo) >> bf_pos(g, (uint32_t)j)) & 1u;
+  return r;
+#endif
 }
 
 __host__ __device__ __forceinline__ uint32_t ceil_log2(uint64_t x) {

@@ -391,10 +391,13 @@ struct Warp {
         const uint32_t sl = d[j];
         bool ok;
         if (MODE == kModeDirectSmem) {
-          ok = (lds_u32(f.bf.smem + (sl >> 5) * 4u) >> (sl & 31u)) & 1u;
+          const uint32_t wd = lds_u32(f.bf.smem + (sl >> 5) * 4u);
+          ok = __funnelshift_r(wd, wd, sl) & 1u;  // rotate right: bit (sl mod 32) to bit 0
         } else if (MODE == kModeBlockedSmem) {
-          const uint2 wv = lds_u32x2(f.bf.smem + bf_word(sl, f.bf.log2) * 8u);
-          ok = bf_test_word<K>(wv.x, wv.y, sl);
+          const uint32_t h1 = bf_h1(sl);
+          const uint32_t w = __funnelshift_rc(h1, 0u, 32u - f.bf.log2);  // h1 >> (32 - log2), 0 for log2 = 0
+          const uint2 wv = lds_u32x2(f.bf.smem + w * 8u);
+          ok = bf_test_word<K>(wv.x, wv.y, bf_g(h1));
         } else if (MODE == kModeBfAny) {
           ok = bf_test(f.bf, sl, pol_keep);
         } else {

@@ -68,6 +68,21 @@ def test_host_columns_form(sj, oracle, engine, small):
     assert got == oracle.run(q, host)
 
 
+def test_host_columns_pinned_streamed(sj, oracle, engine, small, torch_cuda):
+    """Pinned host columns: the first column streams to the device in pieces,
+    the others are read in place at survivor rows."""
+    host, _ = small
+    pinned = {k: torch_cuda.from_numpy(v).pin_memory() for k, v in host.items()}
+    for order, lip, bpk in (((0, 1, 2), True, 16), ((2, 1, 0), True, 0), ((1, 0, 2), False, 0)):
+        q = sj.q33_query(SMALL, order=order, lip=lip, bf_bits_per_key=bpk)
+        got, ms = engine.run(q, pinned, SMALL.fact_rows, host_columns=True)
+        assert got == oracle.run(q, host), (order, lip, bpk)
+        assert ms > 0
+    q = sj.q33_query(SMALL, row_range=(3, 5_999_998), cities=tuple(range(0, 250, 7)), bf_bits_per_key=8)
+    got, _ = engine.run(q, pinned, SMALL.fact_rows, host_columns=True)
+    assert got == oracle.run(q, host)
+
+
 @pytest.mark.parametrize("seed", range(40))
 def test_random_queries(sj, oracle, engine, torch_cuda, seed):
     rng = random.Random(seed)
@@ -180,7 +195,8 @@ def test_bloom_no_false_negatives(sj, engine, torch_cuda, bpk, k):
     f = flags.bool()
     assert bool(out[f].all()), "false negative"
     fpr = out[~f].float().mean().item()
-    bound = {4: 0.45, 8: 0.2, 16: 0.06}[bpk]
+    # k = 1 sets one bit in the low 32-bit half: a 32-bit block
+    bound = ({4: 0.5, 8: 0.3, 16: 0.15} if k == 1 else {4: 0.2, 8: 0.06, 16: 0.02})[bpk]
     assert fpr < bound, fpr
 
 
