@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "libstarjoin.so")
 
-SOURCES = ["sj_engine.cu", "sj_build.cu", "sj_probe.cu", "sj_batch.cu"]
+SOURCES = ["sj_engine.cu", "sj_build.cu", "sj_probe.cu", "sj_batch.cu", "sj_noalloc.cu"]
 HEADERS = ["sj_internal.h", "sj_ptx.cuh", "sj_datagen.h"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",

@@ -132,6 +132,11 @@ def load(build_if_missing: bool = True) -> C.CDLL:
                                            C.c_int32, P]),
         "sj_gen_column_host": (None, [P, C.c_int64, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
                                       C.c_int32, C.c_int]),
+        "sj_ssb_q33_run_noalloc": (C.c_int, [C.c_int] + [P] * 4 + [C.c_int64] + [P] * 2 + [C.c_int64] +
+                                   [P] * 2 + [C.c_int64] + [P] * 2 + [C.c_int64] +
+                                   [P, C.c_int32, C.c_int32, C.POINTER(SjGroupRow), C.c_int64,
+                                    C.POINTER(C.c_int64), P]),
+        "sj_noalloc_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -148,6 +153,7 @@ def exported_symbols() -> List[str]:
         "sj_device_sm_count", "sj_query_prepare", "sj_query_build", "sj_query_probe",
         "sj_query_fetch", "sj_query_get_stats", "sj_query_release", "sj_run_plain",
         "sj_ssb_q33_run", "sj_bloom_test", "sj_gen_column_device", "sj_gen_column_host",
+        "sj_ssb_q33_run_noalloc", "sj_noalloc_last_error",
     ]
 
 

@@ -190,6 +190,29 @@ sj_status sj_ssb_q33_run(sj_engine* e,
                          const int32_t order[3], int32_t lip, int32_t bf_bits_per_key,
                          sj_group_row* out, int64_t cap, int64_t* n_out, float* time_query_ms);
 
+/* The same Q3.3 call for callers that cannot allocate device memory while a
+ * query runs (a fixed device-memory budget handed out up front, an allocator-free
+ * latency path -- cudaMalloc may synchronize the device -- or a runtime that owns
+ * every allocation).  No counterpart in the reference.  It allocates nothing: all
+ * scratch (hash tables, filters, group partials, result rows) lives in one
+ * 48 MiB file-scope device array that every GPU loading this library holds until
+ * the process exits; queries needing more return SJ_ERR_CAPACITY (dimension
+ * tables up to about 1.2M customer + supplier rows fit).  Column pointers are
+ * device memory; `out` is a host buffer of `cap` rows.  The first call on a
+ * device looks up the array's device address (make it before any stream
+ * capture).  Calls share the array and keep the last call's contents (each call
+ * clears what must start at zero); calls that overlap on the GPU race, so
+ * serialize them.  Errors: sj_noalloc_last_error(). */
+sj_status sj_ssb_q33_run_noalloc(int device,
+                                 const int32_t* lo_orderdate, const int32_t* lo_custkey,
+                                 const int32_t* lo_suppkey, const int32_t* lo_revenue, int64_t lo_len,
+                                 const int32_t* d_datekey, const int32_t* d_year, int64_t d_len,
+                                 const int32_t* s_suppkey, const int32_t* s_city, int64_t s_len,
+                                 const int32_t* c_custkey, const int32_t* c_city, int64_t c_len,
+                                 const int32_t order[3], int32_t lip, int32_t bf_bits_per_key,
+                                 sj_group_row* out, int64_t cap, int64_t* n_out, void* stream);
+const char* sj_noalloc_last_error(void);
+
 /* ---- Bloom filter unit interface (tests; the reference's src/ops/bloom.cu) -- */
 /* Build a filter over keys[flags != 0] and probe probe_keys; out_flags[i] = 1 if
  * probe_keys[i] may be present.  All pointers are device pointers.
