@@ -275,14 +275,13 @@ def run_engine(args):
     groups_ok = True
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        # merge the per-rank group partials (24 groups of the Q3.3 shape)
-        dense = torch.zeros(2 * 2 * 7 * 2, dtype=torch.int64, device=f"cuda:{local}")
-        for (s, c, y, cnt, sm) in result:
-            gi = ((0 if s == 231 else 1) * 2 + (0 if c == 231 else 1)) * 7 + (y - 1992)
-            dense[2 * gi] += cnt
-            dense[2 * gi + 1] += sm if sm < 2 ** 63 else sm - 2 ** 64
-        dist.all_reduce(dense)
-        groups_ok = int((dense[0::2] > 0).sum().item()) == 24
+        # the exchange step: merge every rank's group partials (outside the timed loop)
+        import multigpu
+        merged = multigpu.merge_groups(result, 3, dist, device=f"cuda:{local}")
+        # every rank's groups are in the merge, and the merged counts cover every rank's rows
+        mine = {r[:3] for r in result}
+        groups_ok = len(merged) == 24 and mine <= {r[:3] for r in merged} and \
+            sum(r[3] for r in merged) >= sum(r[3] for r in result)
     total_ms, probe_ms = t.tolist()
     ms_per_step = total_ms / args.steps
 
