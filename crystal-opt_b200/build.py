@@ -16,11 +16,11 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "libstarjoin.so")
 
-SOURCES = ["sj_engine.cu", "sj_build.cu", "sj_probe.cu", "sj_batch.cu", "sj_noalloc.cu"]
-HEADERS = ["sj_internal.h", "sj_ptx.cuh", "sj_datagen.h"]
+SOURCES = ["sj_engine.cu", "sj_build.cu", "sj_probe.cu", "sj_batch.cu", "sj_batch_host.cu", "sj_serve.cu",
+           "sj_noalloc.cu"]
+HEADERS = ["sj_internal.h", "sj_ptx.cuh", "sj_datagen.h", "sj_shared.h", "sj_cache.h"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-              "-Xcompiler", "-pthread"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-pthread"]
 
 
 def _nvcc() -> str:
@@ -42,19 +42,35 @@ def _stale(target: str, deps: list[str]) -> bool:
 
 
 def build_engine(force: bool = False, verbose: bool = False) -> str:
-    """Compile csrc/*.cu into _build/libstarjoin.so; return its path."""
+    """Compile csrc/*.cu (one object each, in parallel) and link
+    _build/libstarjoin.so; return its path."""
+    from concurrent.futures import ThreadPoolExecutor
+
     srcs = _sources()
-    deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [
-        os.path.join(ROOT, "include", "starjoin.h")]
-    if not force and not _stale(LIB, deps):
-        return LIB
-    os.makedirs(BUILD, exist_ok=True)
-    tmp = LIB + ".tmp"
-    cmd = [_nvcc(), *GENCODE, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-o", tmp, *srcs]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB)
+    common = [os.path.join(CSRC, h) for h in HEADERS] + [
+        os.path.join(ROOT, "include", "starjoin.h"), os.path.join(ROOT, "include", "starjoin_batch.h")]
+    objdir = os.path.join(BUILD, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    objs = [os.path.join(objdir, os.path.basename(s)[:-3] + ".o") for s in srcs]
+    todo = [(s, o) for s, o in zip(srcs, objs) if force or _stale(o, [s] + common)]
+
+    def compile_one(so):
+        src, obj = so
+        cmd = [_nvcc(), *GENCODE, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-c", "-o", obj + ".tmp", src]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(obj + ".tmp", obj)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as ex:
+        list(ex.map(compile_one, todo))
+    if force or todo or _stale(LIB, objs):
+        tmp = LIB + ".tmp"
+        cmd = [_nvcc(), *GENCODE, "-shared", "-Xcompiler", "-pthread", "-o", tmp, *objs]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, LIB)
     return LIB
 
 

@@ -1,0 +1,565 @@
+// sj_batch.cu -- the shared-scan star join: many queries, one pass over the fact table.
+//
+// Design (the shared-pipeline idea of CJOIN, Candea et al., VLDB 2009, mapped to
+// B200): every dimension keeps one 64-bit word per PHT slot whose bit q says
+// whether query slot q's predicate accepts the dimension row stored in that
+// slot.  A fact row starts with the set of query slots whose row range covers it
+// and ANDs in one word per dimension lookup; the survivors are (row, query)
+// pairs, aggregated into per-query group accumulators.  One fact scan and at
+// most one L2 lookup per (row, dimension) serve every query of the batch.
+//
+// Per query this computes exactly what the reference's probe computes for one
+// query (src/ssb-jo/q33/0-lip.cu:28-112 with the uint64 sum of
+// src/ssb-jo/q31/0-lip.cu:98-113): PHT slot (fk - key_min) mod ht_len
+// (crystal/join.cuh:27), a hit iff the slot holds a qualifying row, the group
+// key from that row's attributes.
+//
+// Kernels
+//   sjb_register_kernel  slot uniqueness check + per-slot attribute tables
+//   sjb_zero_jobs_kernel / sjb_build_kernel
+//                        filter bitmap (one bit per slot) + count/min/max
+//                        statistics for each (dimension, predicate) to build
+//   sjb_layout_kernel    group layout and lookup order on the device (batch)
+//   sjb_zero_groups_kernel, sjb_compose_kernel (bitmaps -> 64-bit slot words)
+//   sjb_probe_kernel     the shared scan
+//   sjb_finalize_kernel  non-empty accumulators -> result rows
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sj_cache.h"
+#include "sj_internal.h"
+#include "sj_shared.h"
+
+namespace sj {
+
+constexpr uint32_t kFull = 0xffffffffu;
+
+// ------------------------------------------------------- registration ----
+__global__ void __launch_bounds__(256) sjb_register_kernel(const __grid_constant__ SjbSchemaRt S, uint32_t d,
+                                                           uint32_t* slot_rows, SjbCounters* ctr) {
+  const SjbDimRt& R = S.dim[d];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < R.rows;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = slot_of(R.key[i], R.key_min, R.len, R.fastmod_m);
+    if (atomicAdd(&slot_rows[s], 1u) != 0u) atomicOr(&ctr->error, kBErrCollision);
+    for (uint32_t a = 0; a < R.n_attrs; ++a) const_cast<int32_t*>(R.slot_attr[a])[s] = R.attr[a][i];
+  }
+}
+
+cudaError_t sjb_launch_register(const SjbSchemaRt& S, uint32_t* slot_rows, SjbCounters* ctr, cudaStream_t st) {
+  for (uint32_t d = 0; d < S.n_dims; ++d) {
+    const int64_t rows = S.dim[d].rows;
+    if (rows <= 0) continue;
+    const uint32_t blocks = (uint32_t)std::min<int64_t>((rows + 255) / 256, 4096);
+    uint64_t off = 0;
+    for (uint32_t e = 0; e < d; ++e) off += S.dim[e].len;
+    sjb_register_kernel<<<blocks, 256, 0, st>>>(S, d, slot_rows + off, ctr);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// --------------------------------------------------------- filter build ----
+__global__ void __launch_bounds__(256) sjb_zero_jobs_kernel(const SjbBatchDesc* __restrict__ D) {
+  const uint32_t j = blockIdx.y;
+  if (j >= D->n_jobs) return;
+  const SjbJob& J = D->jobs[j];
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < J.words; w += gridDim.x * blockDim.x)
+    J.bitmap[w] = 0u;
+  if (blockIdx.x == 0 && threadIdx.x < sizeof(SjbEntryStats) / 4)
+    reinterpret_cast<uint32_t*>(J.stats)[threadIdx.x] = 0u;
+}
+
+__global__ void __launch_bounds__(256) sjb_build_kernel(const __grid_constant__ SjbSchemaRt S,
+                                                        const SjbBatchDesc* __restrict__ D) {
+  const uint32_t j = blockIdx.y;
+  if (j >= D->n_jobs) return;
+  const SjbJob J = D->jobs[j];
+  const SjbDimRt& R = S.dim[J.dim];
+  const uint32_t* inb = J.in_index >= 0 ? D->in_bits[J.in_index] : nullptr;
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t cnt = 0;
+  uint32_t umax[SJB_MAX_ATTRS] = {0, 0, 0, 0}, nmin[SJB_MAX_ATTRS] = {0, 0, 0, 0};
+  // the loop bound is uniform across the warp, so full-warp collectives are safe inside
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < R.rows; i0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = i0 + threadIdx.x;
+    bool ok = i < R.rows;
+    const int32_t key = ok ? R.key[i] : 0;
+    ok = ok && key != 0;  // CAS(slot, 0, 0) never claims a slot (crystal/join.cuh:270)
+    if (ok && J.kind != SJ_PRED_ALL) {
+      const int32_t a = R.attr[J.attr][i];
+      if (J.kind == SJ_PRED_RANGE)
+        ok = a >= J.lo && a <= J.hi;
+      else
+        ok = (uint32_t)a < (uint32_t)SJ_MAX_IN_CODES && ((inb[(uint32_t)a >> 5] >> ((uint32_t)a & 31u)) & 1u);
+    }
+    const uint32_t s = ok ? slot_of(key, R.key_min, R.len, R.fastmod_m) : 0u;
+    const uint32_t w = s >> 5, bit = 1u << (s & 31u);
+    uint32_t pend = __ballot_sync(kFull, ok);
+    while (pend) {  // one atomicOr per distinct bitmap word in the warp
+      const uint32_t leader = __ffs(pend) - 1u;
+      const uint32_t lw = __shfl_sync(kFull, w, leader);
+      const bool mine = ((pend >> lane) & 1u) && w == lw;
+      const uint32_t bits = __reduce_or_sync(kFull, mine ? bit : 0u);
+      if (lane == leader) atomicOr(J.bitmap + lw, bits);
+      pend &= ~__ballot_sync(kFull, mine);
+    }
+    if (ok) {
+      ++cnt;
+#pragma unroll
+      for (uint32_t a = 0; a < SJB_MAX_ATTRS; ++a) {
+        if (a < R.n_attrs) {
+          const uint32_t u = (uint32_t)R.attr[a][i] ^ 0x80000000u;
+          umax[a] = max(umax[a], u);
+          nmin[a] = max(nmin[a], ~u);
+        }
+      }
+    }
+  }
+  cnt = __reduce_add_sync(kFull, cnt);
+#pragma unroll
+  for (uint32_t a = 0; a < SJB_MAX_ATTRS; ++a) {
+    umax[a] = __reduce_max_sync(kFull, umax[a]);
+    nmin[a] = __reduce_max_sync(kFull, nmin[a]);
+  }
+  if (lane == 0 && cnt) {
+    atomicAdd(&J.stats->count, cnt);
+    for (uint32_t a = 0; a < R.n_attrs; ++a) {
+      atomicMax(&J.stats->umax[a], umax[a]);
+      atomicMax(&J.stats->nmin[a], nmin[a]);
+    }
+  }
+}
+
+cudaError_t sjb_launch_build(const SjbSchemaRt& S, const SjbBatchDesc* desc, uint32_t max_jobs,
+                             uint32_t jobs_hint, int sm_count, cudaStream_t st) {
+  if (max_jobs == 0) return cudaSuccess;
+  uint64_t max_len = 1, max_rows = 1;
+  for (uint32_t d = 0; d < S.n_dims; ++d) {
+    max_len = std::max<uint64_t>(max_len, S.dim[d].len);
+    max_rows = std::max<uint64_t>(max_rows, (uint64_t)S.dim[d].rows);
+  }
+  // enough blocks for the largest dimension, fewer per job when many jobs share the GPU
+  const uint32_t per_job = (uint32_t)std::max<uint64_t>(
+      1, std::min<uint64_t>((max_rows + 255) / 256,
+                            (uint64_t)std::max(1, sm_count * 8 / (int)std::max(1u, std::min(jobs_hint, 64u)))));
+  const uint32_t zblocks = (uint32_t)std::min<uint64_t>((max_len / 32 + 256) / 256, 64);
+  sjb_zero_jobs_kernel<<<dim3(zblocks, max_jobs), 256, 0, st>>>(desc);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  sjb_build_kernel<<<dim3(per_job, max_jobs), 256, 0, st>>>(S, desc);
+  return cudaGetLastError();
+}
+
+// --------------------------------------------------------------- layout ----
+// One thread per query computes its group layout; thread 0 then assigns
+// accumulator ranges, shared-memory partials and the lookup order.
+__global__ void __launch_bounds__(kBq) sjb_layout_kernel(const __grid_constant__ SjbSchemaRt S,
+                                                         const SjbBatchDesc* __restrict__ D,
+                                                         SjbStep* __restrict__ out, SjbCounters* ctr) {
+  __shared__ SjbStep st;
+  __shared__ uint32_t s_err;
+  const uint32_t q = threadIdx.x;
+  if (q == 0) s_err = 0;
+  __syncthreads();
+  SjbSlot& sl = st.slot[q];
+  for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) {
+    st.bm[q][d] = nullptr;
+    st.sel[q][d] = 1.f;
+  }
+  sl.b = 0;
+  sl.e = 0;
+  sl.group_base = 0;
+  sl.span = 0;
+  sl.n_g = 0;
+  sl.smem_off = -1;
+  bool act = false;
+  if (q < D->n_queries) {
+    const SjbBatchQuery& Q = D->q[q];
+    const SjbEntryStats* stp[SJ_MAX_DIMS];
+    for (uint32_t k = 0; k < Q.n_preds; ++k) stp[k] = Q.stats[k];
+    const uint32_t err = sjb_group_layout(S, Q, stp, sl, st.sel[q], D->group_capacity);
+    if (err) atomicOr(&s_err, err);
+    for (uint32_t k = 0; k < Q.n_preds; ++k) st.bm[q][Q.dim[k]] = Q.bitmap[k];
+    sl.b = Q.b;
+    sl.e = Q.e;
+    act = sl.span > 0 && Q.e > Q.b;
+  }
+  (void)act;
+  __syncthreads();
+  if (q == 0) {
+    uint64_t active = 0, base = 0;
+    int64_t lo = INT64_MAX, hi = 0;
+    for (int i = 0; i < kBq; ++i) {
+      SjbSlot& s = st.slot[i];
+      if (!(i < (int)D->n_queries && s.span > 0 && s.e > s.b)) continue;
+      s.group_base = base;
+      base += s.span;
+      active |= 1ull << i;
+      lo = min(lo, s.b);
+      hi = max(hi, s.e);
+    }
+    if (base > D->group_capacity) {
+      s_err |= kBErrGroupCapacity;
+      active = 0;
+    }
+    st.active = active;
+    st.seg_b = active ? lo : 0;
+    st.seg_e = active ? hi : 0;
+    st.error = s_err;
+    sjb_step_layout(st, S.n_dims, D->smem_capacity);
+    if (s_err) atomicOr(&ctr->error, s_err);
+  }
+  __syncthreads();
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(&st);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(out);
+  for (uint32_t i = threadIdx.x; i < sizeof(SjbStep) / 4; i += blockDim.x) dst[i] = src[i];
+}
+
+cudaError_t sjb_launch_layout(const SjbSchemaRt& S, const SjbBatchDesc* desc, SjbStep* step, SjbCounters* ctr,
+                              cudaStream_t st) {
+  sjb_layout_kernel<<<1, kBq, 0, st>>>(S, desc, step, ctr);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------- zero / compose ----
+__global__ void __launch_bounds__(256) sjb_zero_groups_kernel(const SjbStep* __restrict__ G, uint64_t mask,
+                                                              SjbAcc* __restrict__ acc) {
+  const uint32_t q = blockIdx.y;
+  if (!((G->active & mask) >> q & 1ull)) return;
+  const SjbSlot& s = G->slot[q];
+  ulonglong2* a = reinterpret_cast<ulonglong2*>(acc + s.group_base);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.span; i += gridDim.x * blockDim.x)
+    a[i] = make_ulonglong2(0ull, 0ull);
+}
+
+cudaError_t sjb_launch_zero_groups(const SjbStep* step, uint64_t zero_mask, SjbAcc* acc, int sm_count,
+                                   cudaStream_t st) {
+  sjb_zero_groups_kernel<<<dim3((uint32_t)std::max(1, sm_count / 8), kBq), 256, 0, st>>>(step, zero_mask, acc);
+  return cudaGetLastError();
+}
+
+// Lane j of a warp owns slot 32*w + j; each query's bitmap word w is read once
+// per warp (broadcast) and its bit j lands in bit q of the lane's mask word.
+__global__ void __launch_bounds__(256) sjb_compose_kernel(const __grid_constant__ SjbSchemaRt S,
+                                                          const SjbStep* __restrict__ G) {
+  const uint32_t d = blockIdx.y;
+  if (d >= S.n_dims) return;
+  const SjbDimRt& R = S.dim[d];
+  const uint64_t use = G->use[d];
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t words = (R.len + 31u) / 32u;
+  const uint32_t warps = gridDim.x * (blockDim.x / 32u);
+  for (uint32_t w = blockIdx.x * (blockDim.x / 32u) + (threadIdx.x >> 5); w < words; w += warps) {
+    uint64_t m = 0;
+    uint64_t u = use;
+    while (u) {
+      const int q = __ffsll((long long)u) - 1;
+      u &= u - 1;
+      const uint32_t bits = __ldg(G->bm[q][d] + w);
+      m |= (uint64_t)((bits >> lane) & 1u) << q;
+    }
+    const uint32_t s = w * 32u + lane;
+    if (s < R.len) R.mask[s] = m;
+  }
+}
+
+cudaError_t sjb_launch_compose(const SjbSchemaRt& S, const SjbStep* step, int sm_count, cudaStream_t st) {
+  uint32_t max_len = 1;
+  for (uint32_t d = 0; d < S.n_dims; ++d) max_len = std::max(max_len, S.dim[d].len);
+  const uint32_t warps = (max_len + 31) / 32;
+  const uint32_t blocks = std::min<uint32_t>((warps + 7) / 8, (uint32_t)sm_count * 8);
+  sjb_compose_kernel<<<dim3(blocks, S.n_dims), 256, 0, st>>>(S, step);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------- probe ----
+constexpr int kTileRows = 128;  // 32 lanes x 4 rows
+
+struct TileCols {
+  int4 fk[SJ_MAX_DIMS];
+  int4 m;
+  int4 sub;
+};
+
+struct PosDim {  // dimension parameters by lookup position
+  const int32_t* col;
+  const uint64_t* mask;
+  uint64_t fastmod_m;
+  uint64_t use;
+  int32_t key_min;
+  uint32_t len;
+};
+
+__device__ __forceinline__ int4 ld_col4(const int32_t* __restrict__ c, int64_t r, int64_t n) {
+  if (r + 4 <= n) return __ldcs(reinterpret_cast<const int4*>(c + r));
+  int4 v = make_int4(0, 0, 0, 0);
+  if (r < n) v.x = __ldcs(c + r);
+  if (r + 1 < n) v.y = __ldcs(c + r + 1);
+  if (r + 2 < n) v.z = __ldcs(c + r + 2);
+  return v;
+}
+
+__device__ __forceinline__ int32_t pick(const int4& v, int j) {
+  return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w;
+}
+
+__device__ __forceinline__ uint32_t pick4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t k) {
+  return k == 0 ? a : k == 1 ? b : k == 2 ? c : d;
+}
+
+__device__ __forceinline__ void tile_masks(const int64_t* s_b, const int64_t* s_e, int64_t r0, uint32_t lane,
+                                           uint64_t& act, uint64_t& full) {
+  const int64_t r1 = r0 + kTileRows;
+  const int64_t b0 = s_b[lane], e0 = s_e[lane], b1 = s_b[lane + 32], e1 = s_e[lane + 32];
+  act = (uint64_t)__ballot_sync(kFull, b0 < r1 && e0 > r0) |
+        ((uint64_t)__ballot_sync(kFull, b1 < r1 && e1 > r0) << 32);
+  full = (uint64_t)__ballot_sync(kFull, b0 <= r0 && e0 >= r1) |
+         ((uint64_t)__ballot_sync(kFull, b1 <= r0 && e1 >= r1) << 32);
+}
+
+template <int NW>
+__global__ void __launch_bounds__(NW * 32, 1)
+    sjb_probe_kernel(const __grid_constant__ SjbSchemaRt S, const SjbStep* __restrict__ G,
+                     SjbAcc* __restrict__ acc, SjbCounters* __restrict__ ctr) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  SjbSlot* s_slot = reinterpret_cast<SjbSlot*>(smem);
+  int64_t* s_b = reinterpret_cast<int64_t*>(smem + sizeof(SjbSlot) * kBq);
+  int64_t* s_e = s_b + kBq;
+  SjbAcc* s_acc = reinterpret_cast<SjbAcc*>(s_e + kBq);
+  __shared__ PosDim s_dim[SJ_MAX_DIMS];
+  __shared__ unsigned long long s_rows;
+
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint64_t active = G->active;
+  const uint32_t n_smem = G->smem_entries;
+  const uint32_t nd = G->n_dims;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(G->slot);
+    uint4* dst = reinterpret_cast<uint4*>(s_slot);
+    for (uint32_t i = tid; i < sizeof(SjbSlot) * kBq / 16; i += blockDim.x) dst[i] = src[i];
+    if (tid < kBq) {
+      const bool a = (active >> tid) & 1ull;
+      s_b[tid] = a ? G->slot[tid].b : INT64_MAX;
+      s_e[tid] = a ? G->slot[tid].e : INT64_MIN;
+    }
+    for (uint32_t i = tid; i < n_smem; i += blockDim.x) s_acc[i] = SjbAcc{0ull, 0ull};
+    if (tid < SJ_MAX_DIMS) {
+      PosDim p{nullptr, nullptr, 0ull, 0ull, 0, 1u};
+      if (tid < nd) {
+        const uint32_t d = G->order[tid];
+        p.col = S.dim[d].fact_fk;
+        p.mask = S.dim[d].mask;
+        p.fastmod_m = S.dim[d].fastmod_m;
+        p.use = G->use[d];
+        p.key_min = S.dim[d].key_min;
+        p.len = S.dim[d].len;
+      }
+      s_dim[tid] = p;
+    }
+    if (tid == 0) s_rows = 0;
+  }
+  __syncthreads();
+
+  const int64_t seg_b = G->seg_b, seg_e = G->seg_e, n = S.fact_rows;
+  const int32_t* __restrict__ meas = S.measure;
+  const int32_t* __restrict__ msub = S.measure_sub;
+  unsigned long long rows_seen = 0;
+  if (active != 0 && seg_e > seg_b) {
+    const int64_t tb = seg_b & ~(int64_t)(kTileRows - 1);
+    const int64_t n_tiles = (seg_e - tb + kTileRows - 1) / kTileRows;
+    const int64_t gw = (int64_t)blockIdx.x * NW + warp, GW = (int64_t)gridDim.x * NW;
+
+    auto load = [&](int64_t t, uint64_t act, TileCols& c) {
+      const int64_t r = tb + t * kTileRows + lane * 4;
+#pragma unroll
+      for (int k = 0; k < SJ_MAX_DIMS; ++k)
+        if (k < (int)nd && (act & s_dim[k].use)) c.fk[k] = ld_col4(s_dim[k].col, r, n);
+      c.m = ld_col4(meas, r, n);
+      if (msub) c.sub = ld_col4(msub, r, n);
+    };
+
+    int64_t t = gw;
+    uint64_t act = 0, full = 0;
+    TileCols cur;
+    cur.m = cur.sub = make_int4(0, 0, 0, 0);
+#pragma unroll
+    for (int k = 0; k < SJ_MAX_DIMS; ++k) cur.fk[k] = make_int4(0, 0, 0, 0);
+    if (t < n_tiles) {
+      tile_masks(s_b, s_e, tb + t * kTileRows, lane, act, full);
+      if (act) load(t, act, cur);
+    }
+    while (t < n_tiles) {
+      // prefetch the next tile while this one is processed
+      const int64_t tn = t + GW;
+      uint64_t actn = 0, fulln = 0;
+      TileCols nxt = cur;
+      if (tn < n_tiles) {
+        tile_masks(s_b, s_e, tb + tn * kTileRows, lane, actn, fulln);
+        if (actn) load(tn, actn, nxt);
+      }
+      if (act) {
+        const int64_t r0 = tb + t * kTileRows;
+        rows_seen += (unsigned long long)(min(r0 + kTileRows, min(seg_e, n)) - max(r0, seg_b));
+        const int64_t rb = r0 + lane * 4;
+        const uint64_t part = act & ~full;
+        uint64_t m[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) m[j] = full;
+        if (part) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            uint64_t p = part;
+            while (p) {
+              const int q = __ffsll((long long)p) - 1;
+              p &= p - 1;
+              if (s_b[q] <= rb + j && rb + j < s_e[q]) m[j] |= 1ull << q;
+            }
+          }
+        }
+        uint32_t sl[SJ_MAX_DIMS][4];
+#pragma unroll
+        for (int k = 0; k < SJ_MAX_DIMS; ++k) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) sl[k][j] = 0u;
+          if (k < (int)nd) {
+            const PosDim P = s_dim[k];
+            uint64_t w[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              w[j] = ~0ull;
+              if (m[j] & P.use) {
+                sl[k][j] = slot_of(pick(cur.fk[k], j), P.key_min, P.len, P.fastmod_m);
+                w[j] = __ldg(reinterpret_cast<const unsigned long long*>(P.mask) + sl[k][j]) | ~P.use;
+              }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) m[j] &= w[j];
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          uint64_t mm = m[j];
+          if (!mm) continue;
+          const int64_t v = (int64_t)pick(cur.m, j) - (msub ? (int64_t)pick(cur.sub, j) : 0);
+          while (mm) {
+            const int q = __ffsll((long long)mm) - 1;
+            mm &= mm - 1;
+            const SjbSlot& Q = s_slot[q];
+            uint32_t g = 0;
+            for (int gi = 0; gi < Q.n_g; ++gi) {
+              const uint32_t s = pick4(sl[0][j], sl[1][j], sl[2][j], sl[3][j], Q.gpos[gi]);
+              const int32_t a = __ldg(Q.gtab[gi] + s);
+              g += (uint32_t)(a - Q.pmin[gi]) * Q.stride[gi];
+            }
+            SjbAcc* dst = Q.smem_off >= 0 ? s_acc + Q.smem_off + g : acc + Q.group_base + g;
+            atomicAdd(&dst->cnt, 1ull);
+            atomicAdd(&dst->sum, (unsigned long long)v);
+          }
+        }
+      }
+      cur = nxt;
+      act = actn;
+      full = fulln;
+      t = tn;
+    }
+  }
+  if (lane == 0 && rows_seen) atomicAdd(&s_rows, rows_seen);
+  __syncthreads();
+  // flush the shared partials
+  uint64_t fl = active;
+  while (fl) {
+    const int q = __ffsll((long long)fl) - 1;
+    fl &= fl - 1;
+    const SjbSlot& Q = s_slot[q];
+    if (Q.smem_off < 0) continue;
+    for (uint32_t i = tid; i < Q.span; i += blockDim.x) {
+      const SjbAcc a = s_acc[Q.smem_off + i];
+      if (a.cnt) {
+        atomicAdd(&acc[Q.group_base + i].cnt, a.cnt);
+        atomicAdd(&acc[Q.group_base + i].sum, a.sum);
+      }
+    }
+  }
+  if (tid == 0 && s_rows) atomicAdd(&ctr->rows_scanned, s_rows);
+}
+
+uint32_t sjb_probe_smem_bytes(uint32_t smem_entries) {
+  return (uint32_t)(sizeof(SjbSlot) * kBq + 2 * sizeof(int64_t) * kBq + sizeof(SjbAcc) * smem_entries);
+}
+
+template <int NW>
+static cudaError_t launch_probe_nw(const SjbSchemaRt& S, const SjbStep* step, SjbAcc* acc, SjbCounters* ctr,
+                                   uint32_t smem_entries, int sm_count, cudaStream_t st) {
+  const uint32_t smem = sjb_probe_smem_bytes(smem_entries);
+  cudaError_t e = cudaFuncSetAttribute(sjb_probe_kernel<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  sjb_probe_kernel<NW><<<sm_count, NW * 32, smem, st>>>(S, step, acc, ctr);
+  return cudaGetLastError();
+}
+
+cudaError_t sjb_launch_probe(const SjbSchemaRt& S, const SjbStep* step, SjbAcc* acc, SjbCounters* ctr,
+                             uint32_t threads, uint32_t smem_entries, int sm_count, cudaStream_t st) {
+  switch (threads) {
+    case 256: return launch_probe_nw<8>(S, step, acc, ctr, smem_entries, sm_count, st);
+    case 512: return launch_probe_nw<16>(S, step, acc, ctr, smem_entries, sm_count, st);
+    case 1024: return launch_probe_nw<32>(S, step, acc, ctr, smem_entries, sm_count, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// -------------------------------------------------------------- finalize ----
+__global__ void __launch_bounds__(256) sjb_finalize_kernel(const SjbStep* __restrict__ G, uint64_t mask,
+                                                           const SjbAcc* __restrict__ acc, sjb_row* __restrict__ out,
+                                                           uint64_t cap, SjbCounters* ctr,
+                                                           const int32_t* __restrict__ slot_query) {
+  const uint32_t q = blockIdx.y;
+  if (!((G->active & mask) >> q & 1ull)) return;
+  const SjbSlot& s = G->slot[q];
+  const uint32_t lane = threadIdx.x & 31u;
+  const int32_t qid = slot_query ? slot_query[q] : (int32_t)q;
+  const uint32_t span = s.span;
+  // `base` is warp-uniform, so the ballot below sees every lane
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < span;
+       base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + lane;
+    SjbAcc a{0ull, 0ull};
+    if (i < span) a = acc[s.group_base + i];
+    const bool keep = a.cnt != 0ull;
+    const uint32_t bal = __ballot_sync(kFull, keep);
+    if (!bal) continue;
+    unsigned long long first = 0;
+    if (lane == 0) first = atomicAdd(&ctr->out_rows, (unsigned long long)__popc(bal));
+    first = __shfl_sync(kFull, first, 0);
+    if (!keep) continue;
+    const uint64_t idx = first + __popc(bal & ((1u << lane) - 1u));
+    if (idx >= cap) continue;
+    sjb_row r;
+    r.query = qid;
+    r.attr[0] = r.attr[1] = r.attr[2] = r.attr[3] = 0;
+    r.pad_ = 0;
+    for (int g = 0; g < s.n_g; ++g)
+      r.attr[s.gk[g]] = s.pmin[g] + (int32_t)((i / s.stride[g]) % s.width[g]);
+    r.count = a.cnt;
+    r.sum = a.sum;
+    out[idx] = r;
+  }
+}
+
+cudaError_t sjb_launch_finalize(const SjbStep* step, uint64_t mask, const SjbAcc* acc, sjb_row* out, uint64_t cap,
+                                SjbCounters* ctr, const int32_t* slot_query, int sm_count, cudaStream_t st) {
+  sjb_finalize_kernel<<<dim3((uint32_t)std::max(1, sm_count / 4), kBq), 256, 0, st>>>(step, mask, acc, out, cap,
+                                                                                       ctr, slot_query);
+  return cudaGetLastError();
+}
+
+}  // namespace sj

@@ -74,13 +74,14 @@ extern "C" const char* sj_status_string(sj_status s) {
 
 extern "C" const char* sj_last_error(void) { return g_last_error.c_str(); }
 
+namespace sj {
+sj_status set_error(sj_status s, const char* msg) {
+  g_last_error = msg;
+  return s;
+}
+}  // namespace sj
+
 // ---------------------------------------------------------------- engine ----
-struct sj_engine {
-  int device = 0;
-  int sm_count = 148;
-  size_t smem_optin = 232448;
-  cudaMemPool_t pool = nullptr;
-};
 
 extern "C" sj_status sj_engine_create(int device, sj_engine** out) {
   if (!out) return fail(SJ_ERR_INVALID_ARGUMENT, "out is NULL");

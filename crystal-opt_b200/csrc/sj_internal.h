@@ -5,7 +5,21 @@
 
 #include "../../include/starjoin.h"
 
+#include <cuda_runtime.h>
+
+// Engine handle of the C ABI (include/starjoin.h): one device, one memory pool.
+struct sj_engine {
+  int device = 0;
+  int sm_count = 148;
+  size_t smem_optin = 232448;
+  cudaMemPool_t pool = nullptr;
+};
+
 namespace sj {
+
+// Sets the calling thread's sj_last_error() text and returns s.
+sj_status set_error(sj_status s, const char* msg);
+
 
 constexpr int kMaxDims = SJ_MAX_DIMS;
 constexpr int kMaxSteps = 2 * SJ_MAX_DIMS;

@@ -1,0 +1,784 @@
+// sj_serve.cu -- the serving loop (include/starjoin_batch.h, sjs_*).
+//
+// A request loop over a resident fact table.  Queries are admitted while query
+// slots (64) and device memory (filter cache + group accumulators, sized from
+// the free HBM at start) allow; each admitted query attaches to a circular
+// shared scan at its current position and leaves once the scan has covered its
+// fact row range, so a query that arrives while others run shares their scan
+// (continuous batching in the sense of shared-scan engines: CJOIN's continuous
+// pipeline, Crescando's ClockScan).  Between scan steps the loop admits new
+// queries, builds the filters the cache lacks, recomposes the 64-bit slot
+// words when the set of queries changed, and returns finished queries' groups.
+//
+// `plain = 1` serves the same requests one at a time through the plain engine
+// (sj_run_plain), the baseline the shared form is measured against.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "sj_cache.h"
+#include "sj_internal.h"
+#include "sj_shared.h"
+
+using namespace sj;
+
+namespace {
+
+double now_s() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Ticket {
+  sjb_query q{};
+  std::vector<int32_t> codes[SJ_MAX_DIMS];
+  uint64_t worst = 0;
+  double submit_s = 0, admit_s = 0, finish_s = 0;
+  int status = SJ_OK;
+  bool done = false;
+  std::vector<sjb_row> rows;
+};
+
+struct Interval {
+  int64_t b, e;
+};
+
+struct Slot {
+  bool used = false;
+  uint64_t ticket = 0;
+  int entry[SJ_MAX_DIMS] = {-1, -1, -1, -1};
+  int n_entries = 0;
+  uint64_t group_off = 0, group_span = 0;
+  SjbSlot lay{};
+  float sel[SJ_MAX_DIMS] = {1.f, 1.f, 1.f, 1.f};
+  const uint32_t* bm[SJ_MAX_DIMS] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<Interval> remaining;  // fact rows still to scan (at most two pieces)
+};
+
+}  // namespace
+
+struct sjs_server {
+  sj_engine* eng = nullptr;
+  SchemaState S;
+  sjs_config cfg{};
+  int64_t step_rows = 0;
+  int max_active = kBq;
+  uint64_t result_rows = 1ull << 20;
+  // device
+  SjbAcc* acc = nullptr;
+  sjb_row* rows_d = nullptr;
+  SjbCounters* ctr_d = nullptr;
+  SjbStep* step_d = nullptr;
+  SjbBatchDesc* desc_d = nullptr;
+  uint8_t* arena = nullptr;
+  SjbEntryStats* stats_d = nullptr;
+  int32_t* slot_query_d = nullptr;
+  // pinned
+  SjbStep* step_h[2] = {nullptr, nullptr};
+  SjbBatchDesc* desc_h = nullptr;
+  SjbCounters* ctr_h = nullptr;
+  SjbEntryStats* stats_h = nullptr;
+  int32_t* slot_query_h = nullptr;
+  cudaStream_t st = nullptr;
+  FilterCache cache;
+  RangeAlloc groups;
+  // loop state
+  std::thread th;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<uint64_t> pending;
+  std::unordered_map<uint64_t, Ticket> tickets;
+  uint64_t next_ticket = 1;
+  bool stop = false;
+  Slot slots[kBq];
+  int64_t pos = 0;
+  bool masks_dirty = true;
+  sjs_stats stats{};
+  std::string loop_error;
+};
+
+namespace {
+
+void finish_ticket(sjs_server* s, uint64_t id, int status, std::vector<sjb_row>&& rows) {
+  std::lock_guard<std::mutex> g(s->mu);
+  auto it = s->tickets.find(id);
+  if (it == s->tickets.end()) return;
+  Ticket& t = it->second;
+  t.status = status;
+  t.rows = std::move(rows);
+  t.finish_s = now_s();
+  t.done = true;
+  ++s->stats.finished;
+  s->cv_done.notify_all();
+}
+
+// Rows [b, e) intersected with the rows still to scan, one piece (the scan
+// never wraps inside a step, so at most one piece is non-empty).
+Interval take(const Slot& sl, int64_t b, int64_t e) {
+  for (const Interval& iv : sl.remaining) {
+    const int64_t lo = std::max(iv.b, b), hi = std::min(iv.e, e);
+    if (lo < hi) return {lo, hi};
+  }
+  return {0, 0};
+}
+
+void cover(Slot& sl, Interval c) {
+  std::vector<Interval> out;
+  for (const Interval& iv : sl.remaining) {
+    if (c.e <= iv.b || c.b >= iv.e) {
+      out.push_back(iv);
+      continue;
+    }
+    if (iv.b < c.b) out.push_back({iv.b, c.b});
+    if (c.e < iv.e) out.push_back({c.e, iv.e});
+  }
+  sl.remaining.swap(out);
+}
+
+// Next row at or after `pos` (cyclically over [0, n)) that an admitted query still needs.
+int64_t next_needed(sjs_server* s, int64_t pos, int64_t n) {
+  int64_t best = -1, best_dist = INT64_MAX;
+  for (const Slot& sl : s->slots) {
+    if (!sl.used) continue;
+    for (const Interval& iv : sl.remaining) {
+      int64_t cand, dist;
+      if (pos >= iv.b && pos < iv.e) {
+        cand = pos;
+        dist = 0;
+      } else if (iv.b >= pos) {
+        cand = iv.b;
+        dist = iv.b - pos;
+      } else {
+        cand = iv.b;
+        dist = iv.b + n - pos;
+      }
+      if (dist < best_dist) {
+        best_dist = dist;
+        best = cand;
+      }
+    }
+  }
+  return best;
+}
+
+void release_slot(sjs_server* s, int q) {
+  Slot& sl = s->slots[q];
+  for (int k = 0; k < sl.n_entries; ++k) s->cache.release(sl.entry[k]);
+  if (sl.group_span) s->groups.release(sl.group_off, sl.group_span);
+  sl = Slot();
+  s->masks_dirty = true;
+}
+
+// Admit pending tickets into free slots while memory allows.  Returns false on a CUDA error.
+bool admit(sjs_server* s) {
+  std::vector<uint64_t> cand;
+  bool idle = true;
+  for (const Slot& sl : s->slots) idle &= !sl.used;
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    int free_slots = 0, used = 0;
+    for (const Slot& sl : s->slots) (sl.used ? used : free_slots) += 1;
+    const int room = std::min(free_slots, s->max_active - used);
+    for (size_t i = 0; i < s->pending.size() && (int)cand.size() < room; ++i) cand.push_back(s->pending[i]);
+  }
+  if (cand.empty()) return true;
+  struct Adm {
+    uint64_t id;
+    int entry[SJ_MAX_DIMS];
+    int n;
+  };
+  std::vector<Adm> adm;
+  SjbBatchDesc& D = *s->desc_h;
+  D.n_jobs = 0;
+  uint32_t n_in = 0;
+  uint64_t hits = 0;
+  std::vector<int> new_ids;
+  for (uint64_t id : cand) {
+    Ticket* t;
+    {
+      std::lock_guard<std::mutex> g(s->mu);
+      t = &s->tickets[id];
+    }
+    Adm a{id, {-1, -1, -1, -1}, 0};
+    bool ok = true;
+    for (int k = 0; k < t->q.n_preds && ok; ++k) {
+      const sjb_pred& p = t->q.preds[k];
+      bool is_new = false;
+      const int eid = s->cache.acquire(p, s->S.words[p.dim], s->cfg.limits.cache_filters != 0, &is_new);
+      if (eid < 0 || (is_new && (D.n_jobs >= (uint32_t)kBMaxJobs ||
+                                 (p.kind == SJ_PRED_IN && n_in >= (uint32_t)kBMaxIn)))) {
+        if (eid >= 0) s->cache.release(eid);
+        ok = false;
+        break;
+      }
+      a.entry[a.n++] = eid;
+      if (is_new) {
+        SjbJob& J = D.jobs[D.n_jobs++];
+        memset(&J, 0, sizeof(J));
+        J.dim = (uint32_t)p.dim;
+        J.attr = p.kind == SJ_PRED_ALL ? -1 : p.attr;
+        J.kind = p.kind;
+        J.lo = p.lo;
+        J.hi = p.hi;
+        J.words = s->S.words[p.dim];
+        J.in_index = -1;
+        if (p.kind == SJ_PRED_IN) {
+          J.in_index = (int32_t)n_in;
+          uint32_t* bits = D.in_bits[n_in++];
+          memset(bits, 0, sizeof(uint32_t) * kBInWords);
+          for (int c = 0; c < p.in_count; ++c) bits[p.in_codes[c] >> 5] |= 1u << (p.in_codes[c] & 31);
+        }
+        J.bitmap = s->cache.bitmap(eid);
+        J.stats = s->cache.stats(eid);
+        new_ids.push_back(eid);
+      } else {
+        ++hits;
+      }
+    }
+    if (!ok) {
+      for (int k = 0; k < a.n; ++k) s->cache.release(a.entry[k]);
+      if (idle && adm.empty()) {  // cannot fit even alone: refuse it
+        {
+          std::lock_guard<std::mutex> g(s->mu);
+          s->pending.erase(std::find(s->pending.begin(), s->pending.end(), id));
+          ++s->stats.rejected;
+        }
+        finish_ticket(s, id, SJ_ERR_REJECTED, {});
+      }
+      break;  // memory is full: keep FIFO order, retry after queries leave
+    }
+    adm.push_back(a);
+  }
+  // build the new filters and read back every admitted predicate's statistics
+  if (D.n_jobs) {
+    if (cudaMemcpyAsync(s->desc_d, s->desc_h, sizeof(SjbBatchDesc), cudaMemcpyHostToDevice, s->st) != cudaSuccess)
+      return false;
+    if (sjb_launch_build(s->S.rt, s->desc_d, D.n_jobs, D.n_jobs, s->eng->sm_count, s->st) != cudaSuccess)
+      return false;
+    for (size_t i = 0; i < new_ids.size(); ++i)
+      if (cudaMemcpyAsync(s->stats_h + i, s->cache.stats(new_ids[i]), sizeof(SjbEntryStats),
+                          cudaMemcpyDeviceToHost, s->st) != cudaSuccess)
+        return false;
+    if (cudaStreamSynchronize(s->st) != cudaSuccess) return false;
+    for (size_t i = 0; i < new_ids.size(); ++i) {
+      FilterEntry& e = s->cache.at(new_ids[i]);
+      e.host = s->stats_h[i];
+      e.host_valid = true;
+      e.built = true;
+    }
+    std::lock_guard<std::mutex> g(s->mu);
+    s->stats.filters_built += new_ids.size();
+  }
+  // group layout and accumulator ranges
+  const double t_adm = now_s();
+  for (const Adm& a : adm) {
+    Ticket* t;
+    {
+      std::lock_guard<std::mutex> g(s->mu);
+      t = &s->tickets[a.id];
+    }
+    SjbBatchQuery bq{};
+    bq.b = t->q.row_begin;
+    bq.e = t->q.row_end;
+    bq.n_preds = (uint32_t)t->q.n_preds;
+    const SjbEntryStats* stp[SJ_MAX_DIMS];
+    for (int k = 0; k < a.n; ++k) {
+      bq.dim[k] = (uint32_t)t->q.preds[k].dim;
+      bq.group_attr[k] = t->q.preds[k].group_attr;
+      stp[k] = &s->cache.at(a.entry[k]).host;
+    }
+    SjbSlot lay{};
+    float sel[SJ_MAX_DIMS] = {1.f, 1.f, 1.f, 1.f};
+    const uint32_t err = sjb_group_layout(s->S.rt, bq, stp, lay, sel, 1ull << 32);
+    const uint64_t span = lay.span;
+    uint64_t off = 0;
+    if (span && !err) {
+      off = s->groups.alloc(span);
+      if (off == ~0ull) {  // accumulators full: this and later tickets wait
+        for (const Adm& rest : adm)
+          if (&rest >= &a)
+            for (int k = 0; k < rest.n; ++k) s->cache.release(rest.entry[k]);
+        bool any = false;
+        for (const Slot& sl : s->slots) any |= sl.used;
+        if (!any) {  // cannot fit even alone: refuse it
+          {
+            std::lock_guard<std::mutex> g(s->mu);
+            s->pending.erase(std::find(s->pending.begin(), s->pending.end(), a.id));
+            ++s->stats.rejected;
+          }
+          finish_ticket(s, a.id, SJ_ERR_REJECTED, {});
+        }
+        break;
+      }
+    }
+    {
+      std::lock_guard<std::mutex> g(s->mu);
+      s->pending.erase(std::find(s->pending.begin(), s->pending.end(), a.id));
+      t->admit_s = t_adm;
+      ++s->stats.admitted;
+    }
+    if (err || span == 0 || bq.e <= bq.b) {  // no row can match (or key space too large)
+      for (int k = 0; k < a.n; ++k) s->cache.release(a.entry[k]);
+      finish_ticket(s, a.id, err ? SJ_ERR_CAPACITY : SJ_OK, {});
+      continue;
+    }
+    int q = 0;
+    while (s->slots[q].used) ++q;
+    Slot& sl = s->slots[q];
+    sl.used = true;
+    sl.ticket = a.id;
+    sl.n_entries = a.n;
+    for (int k = 0; k < a.n; ++k) {
+      sl.entry[k] = a.entry[k];
+      sl.bm[bq.dim[k]] = s->cache.bitmap(a.entry[k]);
+      sl.sel[bq.dim[k]] = sel[bq.dim[k]];
+    }
+    sl.group_off = off;
+    sl.group_span = span;
+    sl.lay = lay;
+    sl.lay.group_base = off;
+    // the scan is at `pos`: rows [pos, e) come first, then [b, pos) after the wrap
+    const int64_t b = bq.b, e = bq.e, p = s->pos;
+    if (p > b && p < e) {
+      sl.remaining = {{p, e}, {b, p}};
+    } else {
+      sl.remaining = {{b, e}};
+    }
+    if (cudaMemsetAsync(s->acc + off, 0, sizeof(SjbAcc) * span, s->st) != cudaSuccess) return false;
+    s->masks_dirty = true;
+  }
+  uint64_t act = 0;
+  for (const Slot& sl : s->slots) act += sl.used;
+  std::lock_guard<std::mutex> g(s->mu);
+  s->stats.filters_cached += hits;
+  s->stats.peak_active = std::max<uint64_t>(s->stats.peak_active, act);
+  return true;
+}
+
+// Fill a step descriptor from the admitted slots; `step` selects which slots
+// are active (rows in this step) -- all admitted slots for mask composition.
+void fill_step(sjs_server* s, SjbStep& st, bool all, int64_t seg_b, int64_t seg_e) {
+  memset(&st, 0, sizeof(SjbStep));
+  st.seg_b = seg_b;
+  st.seg_e = seg_e;
+  uint64_t active = 0;
+  for (int q = 0; q < kBq; ++q) {
+    Slot& sl = s->slots[q];
+    st.slot[q] = sl.lay;
+    st.slot[q].b = st.slot[q].e = 0;
+    for (int d = 0; d < SJ_MAX_DIMS; ++d) {
+      st.bm[q][d] = sl.used ? sl.bm[d] : nullptr;
+      st.sel[q][d] = sl.sel[d];
+    }
+    if (!sl.used) continue;
+    if (all) {
+      active |= 1ull << q;
+      continue;
+    }
+    const Interval iv = take(sl, seg_b, seg_e);
+    if (iv.e > iv.b) {
+      st.slot[q].b = iv.b;
+      st.slot[q].e = iv.e;
+      active |= 1ull << q;
+    }
+  }
+  st.active = active;
+  sjb_step_layout(st, s->S.rt.n_dims, 6144u);
+}
+
+bool run_step(sjs_server* s) {
+  const int64_t n = s->S.rt.fact_rows;
+  if (s->masks_dirty) {
+    fill_step(s, *s->step_h[0], true, 0, 0);
+    if (cudaMemcpyAsync(s->step_d, s->step_h[0], sizeof(SjbStep), cudaMemcpyHostToDevice, s->st) != cudaSuccess)
+      return false;
+    if (sjb_launch_compose(s->S.rt, s->step_d, s->eng->sm_count, s->st) != cudaSuccess) return false;
+    s->masks_dirty = false;
+  }
+  const int64_t p = next_needed(s, s->pos, n);
+  if (p < 0) return true;
+  const int64_t seg_b = p, seg_e = std::min<int64_t>(n, p + s->step_rows);
+  SjbStep& st = *s->step_h[1];
+  fill_step(s, st, false, seg_b, seg_e);
+  if (cudaMemcpyAsync(s->step_d, s->step_h[1], sizeof(SjbStep), cudaMemcpyHostToDevice, s->st) != cudaSuccess)
+    return false;
+  if (cudaMemsetAsync(s->ctr_d, 0, sizeof(SjbCounters), s->st) != cudaSuccess) return false;
+  const uint32_t threads = s->cfg.limits.threads ? (uint32_t)s->cfg.limits.threads : 512u;
+  if (sjb_launch_probe(s->S.rt, s->step_d, s->acc, s->ctr_d, threads, st.smem_entries, s->eng->sm_count, s->st) !=
+      cudaSuccess)
+    return false;
+  // coverage and finished queries
+  uint64_t fin = 0;
+  for (int q = 0; q < kBq; ++q) {
+    Slot& sl = s->slots[q];
+    if (!sl.used || !((st.active >> q) & 1ull)) continue;
+    cover(sl, {st.slot[q].b, st.slot[q].e});
+    if (sl.remaining.empty()) fin |= 1ull << q;
+  }
+  if (fin) {
+    for (int q = 0; q < kBq; ++q) s->slot_query_h[q] = q;
+    if (cudaMemcpyAsync(s->slot_query_d, s->slot_query_h, sizeof(int32_t) * kBq, cudaMemcpyHostToDevice, s->st) !=
+        cudaSuccess)
+      return false;
+    // finalize the finished slots in groups whose spans fit the result buffer
+    uint64_t left = fin;
+    while (left) {
+      uint64_t part = 0, rows = 0;
+      for (int q = 0; q < kBq; ++q) {
+        if (!((left >> q) & 1ull)) continue;
+        const uint64_t sp = s->slots[q].group_span;
+        if (part && rows + sp > s->result_rows) continue;
+        part |= 1ull << q;
+        rows += sp;
+      }
+      left &= ~part;
+      if (cudaMemsetAsync(s->ctr_d + 1, 0, sizeof(SjbCounters), s->st) != cudaSuccess) return false;
+      // the finalize kernel reads slot spans and bases from step_d; keep its active set
+      if (sjb_launch_finalize(s->step_d, part, s->acc, s->rows_d, s->result_rows, s->ctr_d + 1, s->slot_query_d,
+                              s->eng->sm_count, s->st) != cudaSuccess)
+        return false;
+      if (cudaMemcpyAsync(s->ctr_h, s->ctr_d, 2 * sizeof(SjbCounters), cudaMemcpyDeviceToHost, s->st) !=
+          cudaSuccess)
+        return false;
+      if (cudaStreamSynchronize(s->st) != cudaSuccess) return false;
+      const uint64_t nrows = std::min<uint64_t>(s->ctr_h[1].out_rows, s->result_rows);
+      std::vector<sjb_row> all(nrows);
+      if (nrows && cudaMemcpy(all.data(), s->rows_d, sizeof(sjb_row) * nrows, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return false;
+      std::vector<std::vector<sjb_row>> per(kBq);
+      for (const sjb_row& r : all) per[r.query].push_back(r);
+      for (int q = 0; q < kBq; ++q) {
+        if (!((part >> q) & 1ull)) continue;
+        for (sjb_row& r : per[q]) r.query = 0;
+        const uint64_t id = s->slots[q].ticket;
+        release_slot(s, q);
+        finish_ticket(s, id, SJ_OK, std::move(per[q]));
+      }
+    }
+  } else if (cudaMemcpyAsync(s->ctr_h, s->ctr_d, sizeof(SjbCounters), cudaMemcpyDeviceToHost, s->st) !=
+                 cudaSuccess ||
+             cudaStreamSynchronize(s->st) != cudaSuccess) {
+    return false;
+  }
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    s->stats.rows_scanned += s->ctr_h[0].rows_scanned;
+    ++s->stats.steps;
+  }
+  s->pos = seg_e >= n ? 0 : seg_e;
+  return true;
+}
+
+void plain_one(sjs_server* s, uint64_t id) {
+  Ticket* t;
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    s->pending.pop_front();
+    t = &s->tickets[id];
+    t->admit_s = now_s();
+    ++s->stats.admitted;
+  }
+  const sjb_query& q = t->q;
+  sj_plan plan;
+  memset(&plan, 0, sizeof(plan));
+  plan.n_dims = q.n_preds;
+  for (int k = 0; k < q.n_preds; ++k) {
+    const sjb_pred& p = q.preds[k];
+    const sjb_dim& D = s->S.schema.dims[p.dim];
+    sj_dim& d = plan.dims[k];
+    d.fact_fk = D.fact_fk;
+    d.key = D.key;
+    d.filter_attr = p.kind == SJ_PRED_ALL ? nullptr : D.attr[p.attr];
+    d.payload = p.group_attr >= 0 ? D.attr[p.group_attr] : nullptr;
+    d.rows = D.rows;
+    d.key_min = D.key_min;
+    d.ht_len = D.ht_len;
+    d.pred_kind = p.kind;
+    d.pred_lo = p.lo;
+    d.pred_hi = p.hi;
+    d.in_count = p.in_count;
+    d.in_codes = p.in_codes;
+    d.group = p.group_attr >= 0;
+    if (d.group) {
+      d.payload_min = (int32_t)s->S.attr_min[p.dim][p.group_attr];
+      d.payload_max = (int32_t)s->S.attr_max[p.dim][p.group_attr];
+    }
+    plan.order[k] = k;
+  }
+  plan.measure = s->S.schema.measure;
+  plan.measure_sub = s->S.schema.measure_sub;
+  plan.fact_rows = s->S.schema.fact_rows;
+  plan.row_begin = q.row_begin;
+  plan.row_end = q.row_end;
+  plan.lip = 1;
+  plan.bf_bits_per_key = 0;
+  plan.bf_hashes = 2;
+  std::vector<sj_group_row> rows(4096);
+  int64_t n = 0;
+  float ms = 0.f;
+  sj_status rc = sj_run_plain(s->eng, &plan, 0, rows.data(), (int64_t)rows.size(), &n, &ms, s->st);
+  if (rc == SJ_ERR_CAPACITY && n > (int64_t)rows.size()) {
+    rows.resize((size_t)n);
+    rc = sj_run_plain(s->eng, &plan, 0, rows.data(), (int64_t)rows.size(), &n, &ms, s->st);
+  }
+  std::vector<sjb_row> out;
+  if (rc == SJ_OK) {
+    out.resize((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+      sjb_row& r = out[(size_t)i];
+      memset(&r, 0, sizeof(r));
+      for (int k = 0; k < q.n_preds; ++k) r.attr[k] = q.preds[k].group_attr >= 0 ? rows[(size_t)i].attr[k] : 0;
+      r.count = rows[(size_t)i].count;
+      r.sum = rows[(size_t)i].sum;
+    }
+    std::lock_guard<std::mutex> g(s->mu);
+    s->stats.rows_scanned += (uint64_t)(q.row_end - q.row_begin);
+    ++s->stats.steps;
+  }
+  finish_ticket(s, id, rc, std::move(out));
+}
+
+void loop(sjs_server* s) {
+  cudaSetDevice(s->eng->device);
+  for (;;) {
+    bool any_active = false;
+    for (const Slot& sl : s->slots) any_active |= sl.used;
+    {
+      std::unique_lock<std::mutex> g(s->mu);
+      if (!any_active)
+        s->cv_work.wait(g, [&] { return s->stop || !s->pending.empty(); });
+      if (s->stop) break;
+    }
+    const double t0 = now_s();
+    bool ok = true;
+    if (s->cfg.plain) {
+      uint64_t id = 0;
+      {
+        std::lock_guard<std::mutex> g(s->mu);
+        if (!s->pending.empty()) id = s->pending.front();
+      }
+      if (id) plain_one(s, id);
+    } else {
+      ok = admit(s);
+      bool active = false;
+      for (const Slot& sl : s->slots) active |= sl.used;
+      if (ok && active) ok = run_step(s);
+    }
+    {
+      std::lock_guard<std::mutex> g(s->mu);
+      s->stats.busy_s += now_s() - t0;
+    }
+    if (!ok) {  // a CUDA error ends the loop; every waiting ticket fails
+      std::lock_guard<std::mutex> g(s->mu);
+      s->loop_error = cudaGetErrorString(cudaGetLastError());
+      for (auto& kv : s->tickets)
+        if (!kv.second.done) {
+          kv.second.done = true;
+          kv.second.status = SJ_ERR_CUDA;
+          kv.second.finish_s = now_s();
+        }
+      s->pending.clear();
+      s->cv_done.notify_all();
+      break;
+    }
+  }
+}
+
+void server_free(sjs_server* s) {
+  if (!s) return;
+  cudaSetDevice(s->eng->device);
+  if (s->st) cudaStreamSynchronize(s->st);
+  cudaFree(s->acc);
+  cudaFree(s->rows_d);
+  cudaFree(s->ctr_d);
+  cudaFree(s->step_d);
+  cudaFree(s->desc_d);
+  cudaFree(s->arena);
+  cudaFree(s->stats_d);
+  cudaFree(s->slot_query_d);
+  cudaFreeHost(s->step_h[0]);
+  cudaFreeHost(s->step_h[1]);
+  cudaFreeHost(s->desc_h);
+  cudaFreeHost(s->ctr_h);
+  cudaFreeHost(s->stats_h);
+  cudaFreeHost(s->slot_query_h);
+  if (s->st) cudaStreamDestroy(s->st);
+  schema_release(s->S);
+  delete s;
+}
+
+}  // namespace
+
+extern "C" double sjs_now(void) { return now_s(); }
+
+extern "C" sj_status sjs_server_create(sj_engine* eng, const sjb_schema* schema, const sjs_config* cfg,
+                                       sjs_server** out) {
+  if (!eng || !out) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "engine or out is NULL");
+  *out = nullptr;
+  sjs_server* s = new sjs_server();
+  s->eng = eng;
+  if (cfg) s->cfg = *cfg;
+  sj_status rc = schema_register(eng, schema, s->S);
+  if (rc != SJ_OK) {
+    delete s;
+    return rc;
+  }
+  const int64_t n = s->S.rt.fact_rows;
+  s->step_rows = s->cfg.step_rows > 0 ? s->cfg.step_rows : std::max<int64_t>(1 << 20, n / 8);
+  s->step_rows = (s->step_rows + 127) / 128 * 128;
+  s->max_active = s->cfg.max_active > 0 ? std::min(s->cfg.max_active, kBq) : kBq;
+  const uint32_t threads = s->cfg.limits.threads ? (uint32_t)s->cfg.limits.threads : 512u;
+  if (threads != 256 && threads != 512 && threads != 1024) {
+    server_free(s);
+    return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "threads=%d (256, 512 or 1024)", s->cfg.limits.threads);
+  }
+  // admission budget: device memory that is free now, minus the reserve
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const int64_t reserve = s->cfg.hbm_reserve_bytes > 0 ? s->cfg.hbm_reserve_bytes : (2ll << 30);
+  const int64_t budget = std::max<int64_t>(64ll << 20, (int64_t)free_b - reserve);
+  int64_t groups = s->cfg.limits.group_entries > 0 ? s->cfg.limits.group_entries : (1ll << 24);
+  int64_t fcache = s->cfg.limits.filter_cache_bytes > 0 ? s->cfg.limits.filter_cache_bytes : (1ll << 30);
+  groups = std::min<int64_t>(groups, budget / 2 / (int64_t)sizeof(SjbAcc));
+  fcache = std::min<int64_t>(fcache, budget / 2);
+  s->cfg.limits.group_entries = groups;
+  s->cfg.limits.filter_cache_bytes = fcache;
+  cudaError_t e = cudaSuccess;
+  auto step = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+  };
+  const uint32_t max_entries = 8192;
+  step(cudaMalloc(&s->acc, sizeof(SjbAcc) * (size_t)groups));
+  step(cudaMalloc(&s->rows_d, sizeof(sjb_row) * s->result_rows));
+  step(cudaMalloc(&s->ctr_d, 2 * sizeof(SjbCounters)));
+  step(cudaMalloc(&s->step_d, sizeof(SjbStep)));
+  step(cudaMalloc(&s->desc_d, sizeof(SjbBatchDesc)));
+  step(cudaMalloc(&s->arena, (size_t)fcache));
+  step(cudaMalloc(&s->stats_d, sizeof(SjbEntryStats) * max_entries));
+  step(cudaMalloc(&s->slot_query_d, sizeof(int32_t) * kBq));
+  step(cudaMallocHost(&s->step_h[0], sizeof(SjbStep)));
+  step(cudaMallocHost(&s->step_h[1], sizeof(SjbStep)));
+  step(cudaMallocHost(&s->desc_h, sizeof(SjbBatchDesc)));
+  step(cudaMallocHost(&s->ctr_h, 2 * sizeof(SjbCounters)));
+  step(cudaMallocHost(&s->stats_h, sizeof(SjbEntryStats) * kBMaxJobs));
+  step(cudaMallocHost(&s->slot_query_h, sizeof(int32_t) * kBq));
+  step(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  if (e != cudaSuccess) {
+    rc = cuda_fail(e, "sjs_server_create");
+    server_free(s);
+    return rc;
+  }
+  memset(s->desc_h, 0, sizeof(SjbBatchDesc));
+  s->cache.init(s->arena, (uint64_t)fcache, s->stats_d, max_entries);
+  s->groups.reset((uint64_t)groups, 1);
+  s->th = std::thread(loop, s);
+  *out = s;
+  return SJ_OK;
+}
+
+extern "C" sj_status sjs_submit(sjs_server* s, const sjb_query* q, uint64_t* ticket) {
+  if (!s || !q || !ticket) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "NULL argument");
+  uint64_t worst = 0;
+  sj_status rc = validate_query(s->S, *q, &worst);
+  if (rc != SJ_OK) return rc;
+  if (worst > (uint64_t)s->cfg.limits.group_entries || worst > s->result_rows) {
+    std::lock_guard<std::mutex> g(s->mu);
+    ++s->stats.rejected;
+    return fail_fmt(SJ_ERR_REJECTED, "query may need %llu group entries (server holds %lld)",
+                    (unsigned long long)worst, (long long)s->cfg.limits.group_entries);
+  }
+  std::lock_guard<std::mutex> g(s->mu);
+  if (!s->loop_error.empty()) return fail_fmt(SJ_ERR_CUDA, "server stopped: %s", s->loop_error.c_str());
+  const uint64_t id = s->next_ticket++;
+  Ticket& t = s->tickets[id];
+  t.q = *q;
+  for (int k = 0; k < q->n_preds; ++k) {
+    if (q->preds[k].kind == SJ_PRED_IN && q->preds[k].in_count > 0) {
+      t.codes[k].assign(q->preds[k].in_codes, q->preds[k].in_codes + q->preds[k].in_count);
+      t.q.preds[k].in_codes = t.codes[k].data();
+    } else {
+      t.q.preds[k].in_codes = nullptr;
+      t.q.preds[k].in_count = 0;
+    }
+  }
+  t.worst = worst;
+  t.submit_s = now_s();
+  s->pending.push_back(id);
+  ++s->stats.submitted;
+  *ticket = id;
+  s->cv_work.notify_one();
+  return SJ_OK;
+}
+
+static sj_status take_result(sjs_server* s, Ticket& t, uint64_t ticket, sjs_ticket_info* info, sjb_row* out,
+                             int64_t cap) {
+  if (info) {
+    info->done = t.done;
+    info->status = t.status;
+    info->n_rows = (int64_t)t.rows.size();
+    info->submit_s = t.submit_s;
+    info->admit_s = t.admit_s;
+    info->finish_s = t.finish_s;
+  }
+  if (!t.done || !out) return SJ_OK;
+  if ((int64_t)t.rows.size() > cap)
+    return fail_fmt(SJ_ERR_CAPACITY, "ticket has %zu rows, buffer holds %lld", t.rows.size(), (long long)cap);
+  if (!t.rows.empty()) memcpy(out, t.rows.data(), sizeof(sjb_row) * t.rows.size());
+  const int status = t.status;
+  s->tickets.erase(ticket);
+  return status == SJ_OK ? SJ_OK : fail_fmt((sj_status)status, "query failed: %s", sj_status_string((sj_status)status));
+}
+
+extern "C" sj_status sjs_poll(sjs_server* s, uint64_t ticket, sjs_ticket_info* info, sjb_row* out, int64_t cap) {
+  if (!s) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "NULL server");
+  std::lock_guard<std::mutex> g(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "unknown ticket %llu", (unsigned long long)ticket);
+  return take_result(s, it->second, ticket, info, out, cap);
+}
+
+extern "C" sj_status sjs_wait(sjs_server* s, uint64_t ticket, double timeout_s, sjs_ticket_info* info, sjb_row* out,
+                              int64_t cap) {
+  if (!s) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "NULL server");
+  std::unique_lock<std::mutex> g(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "unknown ticket %llu", (unsigned long long)ticket);
+  auto ready = [&] { return it->second.done; };
+  if (timeout_s > 0) {
+    if (!s->cv_done.wait_for(g, std::chrono::duration<double>(timeout_s), ready)) {
+      take_result(s, it->second, ticket, info, nullptr, 0);
+      return fail_fmt(SJ_ERR_TIMEOUT, "ticket %llu not finished after %.3f s", (unsigned long long)ticket, timeout_s);
+    }
+  } else {
+    s->cv_done.wait(g, ready);
+  }
+  return take_result(s, it->second, ticket, info, out, cap);
+}
+
+extern "C" sj_status sjs_get_stats(sjs_server* s, sjs_stats* out) {
+  if (!s || !out) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::lock_guard<std::mutex> g(s->mu);
+  *out = s->stats;
+  return SJ_OK;
+}
+
+extern "C" void sjs_server_destroy(sjs_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->th.joinable()) s->th.join();
+  for (int q = 0; q < kBq; ++q)
+    if (s->slots[q].used) release_slot(s, q);
+  server_free(s);
+}

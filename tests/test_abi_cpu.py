@@ -12,7 +12,7 @@ from conftest import HAS_GPU, ROOT
 def _declared(header):
     text = open(os.path.join(ROOT, "include", header)).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(sj_[a-z0-9_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(sj[bs]?_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_every_declared_symbol_is_exported(sj):
@@ -24,7 +24,10 @@ def test_every_declared_symbol_is_exported(sj):
 
 
 def test_binding_covers_header(sj):
+    import shared_scan
     assert set(_declared("starjoin.h")) <= set(sj.exported_symbols())
+    assert set(_declared("starjoin_batch.h")) <= set(shared_scan.SYMBOLS) | set(sj.exported_symbols())
+    shared_scan.load()  # every binding resolves
 
 
 def test_status_strings(sj):

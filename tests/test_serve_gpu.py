@@ -1,0 +1,122 @@
+"""GPU parity of the serving loop (sjs_*): queries admitted while others run
+share the circular scan; each result equals the oracle, equals the same query
+served alone, and equals the plain one-at-a-time loop."""
+import random
+import threading
+import time
+
+import pytest
+
+import shared_scan as ss
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def star(sj, torch_cuda):
+    sc = sj.StarSchema(seed=0x5EED0006, fact_rows=3_000_017, cust_rows=30_000, supp_rows=2000, part_rows=100_000)
+    dev = sj.gen_device(sc)
+    host = {k: v.cpu().numpy() for k, v in dev.items()}
+    return sc, host, dev
+
+
+def _serve(engine, sc, dev, queries, gaps=None, **kw):
+    srv = ss.Server(engine, sc, dev, **kw)
+    try:
+        tickets = []
+        for i, q in enumerate(queries):
+            if gaps:
+                time.sleep(gaps[i])
+            tickets.append(srv.submit(q))
+        out = [srv.wait(t, timeout_s=120.0) for t in tickets]
+        return [r for r, _ in out], [i for _, i in out], srv.stats()
+    finally:
+        srv.close()
+
+
+def test_burst_matches_oracle_and_shares_the_scan(oracle, engine, star):
+    sc, host, dev = star
+    rng = random.Random(10)
+    qs = [ss.random_query(rng, sc, len_range=(100_000, None)) for _ in range(80)]
+    got, info, st = _serve(engine, sc, dev, qs, step_rows=1 << 19)
+    for i, q in enumerate(qs):
+        assert got[i] == oracle.run(ss.to_plain(sc, q), host), i
+        assert info[i].status == 0 and info[i].finish_s >= info[i].admit_s >= info[i].submit_s
+    assert st.finished == 80 and st.peak_active > 1
+    # shared: far fewer rows read than the queries' ranges add up to
+    assert st.rows_scanned < sum(q["row_range"][1] - q["row_range"][0] for q in qs)
+
+
+def test_alone_and_in_the_mix_are_equal(engine, star):
+    sc, _, dev = star
+    rng = random.Random(11)
+    qs = [ss.random_query(rng, sc, len_range=(200_000, None)) for _ in range(30)]
+    probe = qs[7]
+    alone, _, _ = _serve(engine, sc, dev, [probe], step_rows=1 << 18)
+    # arrivals spread over the scan so queries attach at different positions
+    mix, info, st = _serve(engine, sc, dev, qs, gaps=[rng.uniform(0, 0.004) for _ in qs], step_rows=1 << 18)
+    assert mix[7] == alone[0]
+    assert st.steps > 1
+
+
+def test_plain_loop_gives_the_same_results(engine, star):
+    sc, _, dev = star
+    rng = random.Random(12)
+    qs = [ss.random_query(rng, sc, len_range=(100_000, None)) for _ in range(16)]
+    shared, _, _ = _serve(engine, sc, dev, qs)
+    plain, _, st = _serve(engine, sc, dev, qs, plain=True)
+    assert shared == plain
+    assert st.finished == 16
+
+
+def test_small_memory_admits_in_turn(oracle, engine, star):
+    """A filter cache that holds only a few queries' filters: the rest wait and
+    are admitted as earlier queries leave (admission by device memory)."""
+    sc, host, dev = star
+    rng = random.Random(13)
+    qs = [ss.random_query(rng, sc, len_range=(100_000, None)) for _ in range(20)]
+    got, _, st = _serve(engine, sc, dev, qs, filter_cache_bytes=64 << 10, cache_filters=False,
+                        step_rows=1 << 20)
+    for i, q in enumerate(qs):
+        assert got[i] == oracle.run(ss.to_plain(sc, q), host), i
+    assert st.peak_active < 20
+
+
+def test_refusals(sj, engine, star):
+    sc, _, dev = star
+    srv = ss.Server(engine, sc, dev, group_entries=1000)
+    try:
+        big = {"preds": [{"dim": 0, "kind": "all", "group_attr": 0}, {"dim": 1, "kind": "all", "group_attr": 0}],
+               "row_range": (0, 10)}
+        with pytest.raises(sj.StarJoinError) as e:
+            srv.submit(big)
+        assert e.value.status == sj.SJ_ERR_REJECTED
+        assert srv.stats().rejected == 1
+        ok = {"preds": [{"dim": 3, "kind": "all", "group_attr": 0}], "row_range": (0, 5000)}
+        rows, info = srv.wait(srv.submit(ok), timeout_s=60.0)
+        assert sum(r[-2] for r in rows) == 5000
+    finally:
+        srv.close()
+
+
+def test_concurrent_submitters(oracle, engine, star):
+    sc, host, dev = star
+    srv = ss.Server(engine, sc, dev, step_rows=1 << 19)
+    results = {}
+    try:
+        def client(seed):
+            rng = random.Random(seed)
+            for i in range(6):
+                q = ss.random_query(rng, sc, len_range=(100_000, None))
+                rows, _ = srv.wait(srv.submit(q), timeout_s=120.0)
+                results[(seed, i)] = (q, rows)
+        th = [threading.Thread(target=client, args=(s,)) for s in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+    finally:
+        srv.close()
+    assert len(results) == 24
+    for q, rows in results.values():
+        assert rows == oracle.run(ss.to_plain(sc, q), host)
