@@ -190,6 +190,32 @@ def _reference_cuda(args):
             "groups": len(rec["groups"])}
 
 
+def _bf_sweep(eng, schema, cols, args, sptr, stream, torch):
+    """Probe time of the same query with each filter kind (config: direct bitmap,
+    8 and 16 bits per inserted key), every join order of the reference's drivers
+    for the chosen filter."""
+    import starjoin as sj
+    out = {}
+    for bpk in (0, 8, 16):
+        for order in ((0, 1, 2), (2, 1, 0), (1, 2, 0)):
+            q = sj.q33_query(schema, order=order, lip=True, bf_bits_per_key=bpk, bf_hashes=2, adaptive=True)
+            pq = eng.prepare(q, cols, FACT_ROWS)
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(30)]
+            for _ in range(5):
+                pq.build(sptr)
+                pq.probe(sptr)
+            for a, b in evs:
+                pq.build(sptr)
+                a.record(stream)
+                pq.probe(sptr)
+                b.record(stream)
+            torch.cuda.synchronize()
+            ms = statistics.median(a.elapsed_time(b) for a, b in evs)
+            out[f"bpk{bpk}_order{''.join(map(str, order))}_probe_ms"] = ms
+            pq.release()
+    return out
+
+
 def _config(bpk):
     return {"workload": f"3-dim LIP star join, SSB Q3.3 shape: {FACT_ROWS / 1e6:g}M fact rows (fk_cust U[1,600000], "
                         "fk_supp U[1,40000], fk_date over 2556 days, revenue U[1,1e7]); s_city/c_city IN "
@@ -312,8 +338,17 @@ def run_engine(args):
         if world == 1 and not args.no_cpu_baseline:
             host = {k: v.cpu().numpy() for k, v in cols.items()}
             line["cpu_baseline"] = cpu_baseline(host, query)
-        print(json.dumps(line), flush=True)
+        if world == 1 and not args.no_shared:
+            line["bf_sweep"] = _bf_sweep(eng, schema, cols, args, sptr, stream, torch)
     pq.release()
+    if rank == 0 and world == 1 and not args.no_shared:
+        import shared_bench as sb
+        del cols
+        torch.cuda.empty_cache()
+        line["batched"] = sb.batched(eng, n_batches=args.batches)
+        line["serving"] = sb.serving(eng)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:
         dist.destroy_process_group()
@@ -367,18 +402,45 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--bpk", type=int, default=16, help="Bloom bits per inserted key (0 = direct bitmap)")
+    ap.add_argument("--bpk", type=int, default=0,
+                    help="filter: 0 = direct bitmap, one bit per key slot (the reference drivers' sizing, "
+                         "src/ssb-jo/q33/0-lip.cu:221-223); >0 = blocked Bloom filter, bits per inserted key")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--rows", type=int, default=FACT_ROWS,
                     help="fact rows (default: the 120M-row workload; smaller values only for profiling captures)")
+    ap.add_argument("--no-shared", action="store_true", help="skip the batched / serving measurements")
+    ap.add_argument("--shared", choices=["batch", "serve"],
+                    help="run only the batched or the serving measurement (--rows sets the fact table)")
+    ap.add_argument("--batches", type=int, default=6, help="timed batches of the batched measurement")
     args = ap.parse_args()
     FACT_ROWS = args.rows
     args.warmup = max(3, args.warmup)
-    if args.impl == "reference":
+    if args.shared:
+        run_shared(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_engine(args)
+
+
+def run_shared(args):
+    """The shared-scan forms alone (for diagnostics and profiling captures)."""
+    import starjoin as sj
+    import shared_bench as sb
+    eng = sj.Engine(0)
+    if args.shared == "batch":
+        schema = dict(sb.BATCH_SCHEMA)
+        if args.rows != 120_000_000:
+            schema["fact_rows"] = args.rows
+        out = {"batched": sb.batched(eng, n_batches=args.batches, schema=schema)}
+    else:
+        schema = dict(sb.SERVE_SCHEMA)
+        if args.rows != 120_000_000:
+            schema["fact_rows"] = args.rows
+        out = {"serving": sb.serving(eng, schema=schema)}
+    print(json.dumps(out), flush=True)
+    eng.close()
 
 
 if __name__ == "__main__":

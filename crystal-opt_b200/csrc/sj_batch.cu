@@ -182,7 +182,6 @@ __global__ void __launch_bounds__(kBq) sjb_layout_kernel(const __grid_constant__
   sl.span = 0;
   sl.n_g = 0;
   sl.smem_off = -1;
-  bool act = false;
   if (q < D->n_queries) {
     const SjbBatchQuery& Q = D->q[q];
     const SjbEntryStats* stp[SJ_MAX_DIMS];
@@ -192,9 +191,7 @@ __global__ void __launch_bounds__(kBq) sjb_layout_kernel(const __grid_constant__
     for (uint32_t k = 0; k < Q.n_preds; ++k) st.bm[q][Q.dim[k]] = Q.bitmap[k];
     sl.b = Q.b;
     sl.e = Q.e;
-    act = sl.span > 0 && Q.e > Q.b;
   }
-  (void)act;
   __syncthreads();
   if (q == 0) {
     uint64_t active = 0, base = 0;
@@ -248,8 +245,9 @@ cudaError_t sjb_launch_zero_groups(const SjbStep* step, uint64_t zero_mask, SjbA
   return cudaGetLastError();
 }
 
-// Lane j of a warp owns slot 32*w + j; each query's bitmap word w is read once
-// per warp (broadcast) and its bit j lands in bit q of the lane's mask word.
+// Lane j of a warp owns slot 32*w + j.  Lanes first load the bitmap word w of
+// query slots j and j + 32 in parallel; each query's word then reaches every
+// lane by shuffle, and its bit j lands in bit q of lane j's mask word.
 __global__ void __launch_bounds__(256) sjb_compose_kernel(const __grid_constant__ SjbSchemaRt S,
                                                           const SjbStep* __restrict__ G) {
   const uint32_t d = blockIdx.y;
@@ -259,17 +257,19 @@ __global__ void __launch_bounds__(256) sjb_compose_kernel(const __grid_constant_
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t words = (R.len + 31u) / 32u;
   const uint32_t warps = gridDim.x * (blockDim.x / 32u);
+  const uint32_t* bm_lo = ((use >> lane) & 1ull) ? G->bm[lane][d] : nullptr;
+  const uint32_t* bm_hi = ((use >> (lane + 32)) & 1ull) ? G->bm[lane + 32][d] : nullptr;
   for (uint32_t w = blockIdx.x * (blockDim.x / 32u) + (threadIdx.x >> 5); w < words; w += warps) {
-    uint64_t m = 0;
-    uint64_t u = use;
-    while (u) {
-      const int q = __ffsll((long long)u) - 1;
-      u &= u - 1;
-      const uint32_t bits = __ldg(G->bm[q][d] + w);
-      m |= (uint64_t)((bits >> lane) & 1u) << q;
+    const uint32_t lo = bm_lo ? __ldg(bm_lo + w) : 0u;
+    const uint32_t hi = bm_hi ? __ldg(bm_hi + w) : 0u;
+    uint32_t m_lo = 0, m_hi = 0;
+#pragma unroll 8
+    for (int q = 0; q < 32; ++q) {
+      m_lo |= ((__shfl_sync(kFull, lo, q) >> lane) & 1u) << q;
+      m_hi |= ((__shfl_sync(kFull, hi, q) >> lane) & 1u) << q;
     }
     const uint32_t s = w * 32u + lane;
-    if (s < R.len) R.mask[s] = m;
+    if (s < R.len) R.mask[s] = (uint64_t)m_lo | ((uint64_t)m_hi << 32);
   }
 }
 
@@ -327,7 +327,9 @@ __device__ __forceinline__ void tile_masks(const int64_t* s_b, const int64_t* s_
          ((uint64_t)__ballot_sync(kFull, b1 <= r0 && e1 >= r1) << 32);
 }
 
-template <int NW>
+// PF: load the next tile's columns into registers while this tile is processed
+// (for CTAs of 8 or 16 warps); without it, 32 warps per SM hide the latency.
+template <int NW, bool PF>
 __global__ void __launch_bounds__(NW * 32, 1)
     sjb_probe_kernel(const __grid_constant__ SjbSchemaRt S, const SjbStep* __restrict__ G,
                      SjbAcc* __restrict__ acc, SjbCounters* __restrict__ ctr) {
@@ -399,13 +401,15 @@ __global__ void __launch_bounds__(NW * 32, 1)
       if (act) load(t, act, cur);
     }
     while (t < n_tiles) {
-      // prefetch the next tile while this one is processed
       const int64_t tn = t + GW;
       uint64_t actn = 0, fulln = 0;
-      TileCols nxt = cur;
-      if (tn < n_tiles) {
-        tile_masks(s_b, s_e, tb + tn * kTileRows, lane, actn, fulln);
-        if (actn) load(tn, actn, nxt);
+      TileCols nxt;
+      if (PF) {
+        nxt = cur;
+        if (tn < n_tiles) {
+          tile_masks(s_b, s_e, tb + tn * kTileRows, lane, actn, fulln);
+          if (actn) load(tn, actn, nxt);
+        }
       }
       if (act) {
         const int64_t r0 = tb + t * kTileRows;
@@ -426,11 +430,10 @@ __global__ void __launch_bounds__(NW * 32, 1)
             }
           }
         }
-        uint32_t sl[SJ_MAX_DIMS][4];
+        // Lookups in order, most selective dimension first; a row stops at the
+        // first dimension that leaves it no query.
 #pragma unroll
         for (int k = 0; k < SJ_MAX_DIMS; ++k) {
-#pragma unroll
-          for (int j = 0; j < 4; ++j) sl[k][j] = 0u;
           if (k < (int)nd) {
             const PosDim P = s_dim[k];
             uint64_t w[4];
@@ -438,8 +441,8 @@ __global__ void __launch_bounds__(NW * 32, 1)
             for (int j = 0; j < 4; ++j) {
               w[j] = ~0ull;
               if (m[j] & P.use) {
-                sl[k][j] = slot_of(pick(cur.fk[k], j), P.key_min, P.len, P.fastmod_m);
-                w[j] = __ldg(reinterpret_cast<const unsigned long long*>(P.mask) + sl[k][j]) | ~P.use;
+                const uint32_t sk = slot_of(pick(cur.fk[k], j), P.key_min, P.len, P.fastmod_m);
+                w[j] = __ldg(reinterpret_cast<const unsigned long long*>(P.mask) + sk) | ~P.use;
               }
             }
 #pragma unroll
@@ -457,7 +460,12 @@ __global__ void __launch_bounds__(NW * 32, 1)
             const SjbSlot& Q = s_slot[q];
             uint32_t g = 0;
             for (int gi = 0; gi < Q.n_g; ++gi) {
-              const uint32_t s = pick4(sl[0][j], sl[1][j], sl[2][j], sl[3][j], Q.gpos[gi]);
+              // the slot is recomputed here (survivors only) rather than kept per row
+              const uint32_t pos = Q.gpos[gi];
+              const int32_t fk = (int32_t)pick4((uint32_t)pick(cur.fk[0], j), (uint32_t)pick(cur.fk[1], j),
+                                                (uint32_t)pick(cur.fk[2], j), (uint32_t)pick(cur.fk[3], j), pos);
+              const PosDim& P = s_dim[pos];
+              const uint32_t s = slot_of(fk, P.key_min, P.len, P.fastmod_m);
               const int32_t a = __ldg(Q.gtab[gi] + s);
               g += (uint32_t)(a - Q.pmin[gi]) * Q.stride[gi];
             }
@@ -467,9 +475,14 @@ __global__ void __launch_bounds__(NW * 32, 1)
           }
         }
       }
-      cur = nxt;
-      act = actn;
-      full = fulln;
+      if (PF) {
+        cur = nxt;
+        act = actn;
+        full = fulln;
+      } else if (tn < n_tiles) {
+        tile_masks(s_b, s_e, tb + tn * kTileRows, lane, act, full);
+        if (act) load(tn, act, cur);
+      }
       t = tn;
     }
   }
@@ -497,22 +510,22 @@ uint32_t sjb_probe_smem_bytes(uint32_t smem_entries) {
   return (uint32_t)(sizeof(SjbSlot) * kBq + 2 * sizeof(int64_t) * kBq + sizeof(SjbAcc) * smem_entries);
 }
 
-template <int NW>
+template <int NW, bool PF>
 static cudaError_t launch_probe_nw(const SjbSchemaRt& S, const SjbStep* step, SjbAcc* acc, SjbCounters* ctr,
                                    uint32_t smem_entries, int sm_count, cudaStream_t st) {
   const uint32_t smem = sjb_probe_smem_bytes(smem_entries);
-  cudaError_t e = cudaFuncSetAttribute(sjb_probe_kernel<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = cudaFuncSetAttribute(sjb_probe_kernel<NW, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  sjb_probe_kernel<NW><<<sm_count, NW * 32, smem, st>>>(S, step, acc, ctr);
+  sjb_probe_kernel<NW, PF><<<sm_count, NW * 32, smem, st>>>(S, step, acc, ctr);
   return cudaGetLastError();
 }
 
 cudaError_t sjb_launch_probe(const SjbSchemaRt& S, const SjbStep* step, SjbAcc* acc, SjbCounters* ctr,
                              uint32_t threads, uint32_t smem_entries, int sm_count, cudaStream_t st) {
   switch (threads) {
-    case 256: return launch_probe_nw<8>(S, step, acc, ctr, smem_entries, sm_count, st);
-    case 512: return launch_probe_nw<16>(S, step, acc, ctr, smem_entries, sm_count, st);
-    case 1024: return launch_probe_nw<32>(S, step, acc, ctr, smem_entries, sm_count, st);
+    case 256: return launch_probe_nw<8, true>(S, step, acc, ctr, smem_entries, sm_count, st);
+    case 512: return launch_probe_nw<16, true>(S, step, acc, ctr, smem_entries, sm_count, st);
+    case 1024: return launch_probe_nw<32, false>(S, step, acc, ctr, smem_entries, sm_count, st);
   }
   return cudaErrorInvalidValue;
 }

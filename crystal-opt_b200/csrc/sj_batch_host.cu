@@ -279,7 +279,7 @@ extern "C" sj_status sjb_batch_create(sj_engine* eng, const sjb_schema* schema, 
   if (L.group_entries <= 0) L.group_entries = 1ll << 24;
   if (L.result_rows <= 0) L.result_rows = 1ll << 20;
   if (L.filter_cache_bytes <= 0) L.filter_cache_bytes = 1ll << 30;
-  b->threads = L.threads ? (uint32_t)L.threads : 512u;
+  b->threads = L.threads ? (uint32_t)L.threads : 1024u;
   if (b->threads != 256 && b->threads != 512 && b->threads != 1024) {
     delete b;
     return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "threads=%d (256, 512 or 1024)", L.threads);
@@ -340,9 +340,9 @@ static cudaError_t batch_enqueue(sjb_batch* b, cudaStream_t st) {
   SJB_Q(sjb_launch_layout(b->S.rt, b->desc_d, b->step_d, b->ctr_d, st));
   SJB_Q(sjb_launch_zero_groups(b->step_d, ~0ull, b->acc, sm, st));
   SJB_Q(sjb_launch_compose(b->S.rt, b->step_d, sm, st));
-  SJB_Q(cudaEventRecord(b->ev[1], st));
+  SJB_Q(cudaEventRecordWithFlags(b->ev[1], st, b->lim.use_graph ? cudaEventRecordExternal : cudaEventRecordDefault));
   SJB_Q(sjb_launch_probe(b->S.rt, b->step_d, b->acc, b->ctr_d, b->threads, b->smem_entries, sm, st));
-  SJB_Q(cudaEventRecord(b->ev[2], st));
+  SJB_Q(cudaEventRecordWithFlags(b->ev[2], st, b->lim.use_graph ? cudaEventRecordExternal : cudaEventRecordDefault));
   SJB_Q(sjb_launch_finalize(b->step_d, ~0ull, b->acc, b->rows_d, (uint64_t)b->lim.result_rows, b->ctr_d, nullptr,
                             sm, st));
   SJB_Q(cudaMemcpyAsync(b->ctr_h, b->ctr_d, sizeof(SjbCounters), cudaMemcpyDeviceToHost, st));

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -259,18 +260,24 @@ bool admit(sjs_server* s) {
   }
   // build the new filters and read back every admitted predicate's statistics
   if (D.n_jobs) {
-    if (cudaMemcpyAsync(s->desc_d, s->desc_h, sizeof(SjbBatchDesc), cudaMemcpyHostToDevice, s->st) != cudaSuccess)
+    // upload the header and the jobs in use, then the IN-code bitmaps in use
+    const size_t head = offsetof(SjbBatchDesc, jobs) + sizeof(SjbJob) * D.n_jobs;
+    if (cudaMemcpyAsync(s->desc_d, s->desc_h, head, cudaMemcpyHostToDevice, s->st) != cudaSuccess) return false;
+    if (n_in && cudaMemcpyAsync(s->desc_d->in_bits, s->desc_h->in_bits, sizeof(uint32_t) * kBInWords * n_in,
+                                cudaMemcpyHostToDevice, s->st) != cudaSuccess)
       return false;
     if (sjb_launch_build(s->S.rt, s->desc_d, D.n_jobs, D.n_jobs, s->eng->sm_count, s->st) != cudaSuccess)
       return false;
-    for (size_t i = 0; i < new_ids.size(); ++i)
-      if (cudaMemcpyAsync(s->stats_h + i, s->cache.stats(new_ids[i]), sizeof(SjbEntryStats),
-                          cudaMemcpyDeviceToHost, s->st) != cudaSuccess)
-        return false;
+    // one read-back of the statistics records (indexed by entry id)
+    uint32_t hi = 0;
+    for (int id : new_ids) hi = std::max(hi, s->cache.at(id).stats_idx + 1);
+    if (cudaMemcpyAsync(s->stats_h, s->stats_d, sizeof(SjbEntryStats) * hi, cudaMemcpyDeviceToHost, s->st) !=
+        cudaSuccess)
+      return false;
     if (cudaStreamSynchronize(s->st) != cudaSuccess) return false;
     for (size_t i = 0; i < new_ids.size(); ++i) {
       FilterEntry& e = s->cache.at(new_ids[i]);
-      e.host = s->stats_h[i];
+      e.host = s->stats_h[e.stats_idx];
       e.host_valid = true;
       e.built = true;
     }
@@ -411,7 +418,7 @@ bool run_step(sjs_server* s) {
   if (cudaMemcpyAsync(s->step_d, s->step_h[1], sizeof(SjbStep), cudaMemcpyHostToDevice, s->st) != cudaSuccess)
     return false;
   if (cudaMemsetAsync(s->ctr_d, 0, sizeof(SjbCounters), s->st) != cudaSuccess) return false;
-  const uint32_t threads = s->cfg.limits.threads ? (uint32_t)s->cfg.limits.threads : 512u;
+  const uint32_t threads = s->cfg.limits.threads ? (uint32_t)s->cfg.limits.threads : 1024u;
   if (sjb_launch_probe(s->S.rt, s->step_d, s->acc, s->ctr_d, threads, st.smem_entries, s->eng->sm_count, s->st) !=
       cudaSuccess)
     return false;
@@ -568,9 +575,13 @@ void loop(sjs_server* s) {
       if (id) plain_one(s, id);
     } else {
       ok = admit(s);
+      const double t1 = now_s();
       bool active = false;
       for (const Slot& sl : s->slots) active |= sl.used;
       if (ok && active) ok = run_step(s);
+      std::lock_guard<std::mutex> g(s->mu);
+      s->stats.admit_s += t1 - t0;
+      s->stats.scan_s += now_s() - t1;
     }
     {
       std::lock_guard<std::mutex> g(s->mu);
@@ -635,7 +646,7 @@ extern "C" sj_status sjs_server_create(sj_engine* eng, const sjb_schema* schema,
   s->step_rows = s->cfg.step_rows > 0 ? s->cfg.step_rows : std::max<int64_t>(1 << 20, n / 8);
   s->step_rows = (s->step_rows + 127) / 128 * 128;
   s->max_active = s->cfg.max_active > 0 ? std::min(s->cfg.max_active, kBq) : kBq;
-  const uint32_t threads = s->cfg.limits.threads ? (uint32_t)s->cfg.limits.threads : 512u;
+  const uint32_t threads = s->cfg.limits.threads ? (uint32_t)s->cfg.limits.threads : 1024u;
   if (threads != 256 && threads != 512 && threads != 1024) {
     server_free(s);
     return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "threads=%d (256, 512 or 1024)", s->cfg.limits.threads);
@@ -668,7 +679,7 @@ extern "C" sj_status sjs_server_create(sj_engine* eng, const sjb_schema* schema,
   step(cudaMallocHost(&s->step_h[1], sizeof(SjbStep)));
   step(cudaMallocHost(&s->desc_h, sizeof(SjbBatchDesc)));
   step(cudaMallocHost(&s->ctr_h, 2 * sizeof(SjbCounters)));
-  step(cudaMallocHost(&s->stats_h, sizeof(SjbEntryStats) * kBMaxJobs));
+  step(cudaMallocHost(&s->stats_h, sizeof(SjbEntryStats) * max_entries));
   step(cudaMallocHost(&s->slot_query_h, sizeof(int32_t) * kBq));
   step(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
   if (e != cudaSuccess) {

@@ -73,7 +73,7 @@ class SjsStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("finished", C.c_uint64),
                 ("rejected", C.c_uint64), ("steps", C.c_uint64), ("rows_scanned", C.c_uint64),
                 ("filters_built", C.c_uint64), ("filters_cached", C.c_uint64), ("peak_active", C.c_uint64),
-                ("busy_s", C.c_double)]
+                ("busy_s", C.c_double), ("admit_s", C.c_double), ("scan_s", C.c_double)]
 
 
 SYMBOLS = ["sjb_batch_create", "sjb_batch_destroy", "sjb_batch_run", "sjb_batch_get_stats",
@@ -291,15 +291,27 @@ class Batch:
         self.result_rows = result_rows or (1 << 20)
         self._rows = (SjbRow * self.result_rows)()
 
-    def run(self, queries: Sequence[Dict[str, Any]], stream=None) -> List[List[tuple]]:
+    def describe(self, queries: Sequence[Dict[str, Any]]):
+        """The C descriptions of a batch (kept alive by the returned tuple)."""
         arr = (SjbQuery * len(queries))()
         keep: list = []
         for i, q in enumerate(queries):
             fill_query(q, arr[i], keep)
+        return arr, keep
+
+    def run_raw(self, described, stream=None) -> int:
+        """One sjb_batch_run call on a described batch; returns the row count
+        (rows stay in the internal buffer until the next call)."""
+        arr, _ = described
         n = C.c_int64()
-        sj.check(self.lib.sjb_batch_run(self.h, arr, len(queries), self._rows, self.result_rows, C.byref(n),
-                                        stream))
-        return rows_by_query(self._rows, n.value, queries)
+        sj.check(self.lib.sjb_batch_run(self.h, arr, len(arr), self._rows, self.result_rows, C.byref(n), stream))
+        return n.value
+
+    def rows(self, n: int, queries: Sequence[Dict[str, Any]]) -> List[List[tuple]]:
+        return rows_by_query(self._rows, n, queries)
+
+    def run(self, queries: Sequence[Dict[str, Any]], stream=None) -> List[List[tuple]]:
+        return self.rows(self.run_raw(self.describe(queries), stream), queries)
 
     def stats(self) -> SjbStats:
         s = SjbStats()

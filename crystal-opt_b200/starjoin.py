@@ -76,6 +76,16 @@ class SjPlan(C.Structure):
     ]
 
 
+class SjAutotuneOpts(C.Structure):
+    _fields_ = [("reps", C.c_int32), ("tune_filter", C.c_int32), ("tune_order", C.c_int32), ("verify", C.c_int32),
+                ("cache_path", C.c_char_p)]
+
+
+class SjAutotuneReport(C.Structure):
+    _fields_ = [("candidates", C.c_int32), ("cache_hit", C.c_int32), ("mismatches", C.c_int32),
+                ("default_ms", C.c_float), ("best_ms", C.c_float), ("selectivity", C.c_double * MAX_DIMS)]
+
+
 class SjGroupRow(C.Structure):
     _fields_ = [("attr", C.c_int32 * MAX_DIMS), ("count", C.c_uint64), ("sum", C.c_uint64)]
 
@@ -137,6 +147,7 @@ def load(build_if_missing: bool = True) -> C.CDLL:
                                    [P, C.c_int32, C.c_int32, C.POINTER(SjGroupRow), C.c_int64,
                                     C.POINTER(C.c_int64), P]),
         "sj_noalloc_last_error": (C.c_char_p, []),
+        "sj_autotune": (C.c_int, [P, C.POINTER(SjPlan), C.POINTER(SjAutotuneOpts), C.POINTER(SjAutotuneReport), P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -153,7 +164,7 @@ def exported_symbols() -> List[str]:
         "sj_device_sm_count", "sj_query_prepare", "sj_query_build", "sj_query_probe",
         "sj_query_fetch", "sj_query_get_stats", "sj_query_release", "sj_run_plain",
         "sj_ssb_q33_run", "sj_bloom_test", "sj_gen_column_device", "sj_gen_column_host",
-        "sj_ssb_q33_run_noalloc", "sj_noalloc_last_error",
+        "sj_ssb_q33_run_noalloc", "sj_noalloc_last_error", "sj_autotune",
     ]
 
 
@@ -352,6 +363,22 @@ class Engine:
         check(self.lib.sj_run_plain(self.h, C.byref(plan), 1 if host_columns else 0, rows, cap, C.byref(n),
                                     C.byref(ms), stream))
         return rows_to_list(rows, n.value, query), ms.value
+
+    def autotune(self, query, cols, fact_rows, reps=5, tune_filter=False, tune_order=0, verify=True,
+                 cache_path=None, stream=None):
+        """sj_autotune: returns (query with the chosen filter / order, chosen tuning
+        dict, SjAutotuneReport)."""
+        plan, keep = fill_plan(query, cols, fact_rows)
+        opts = SjAutotuneOpts(reps, 1 if tune_filter else 0, tune_order, 1 if verify else 0,
+                              cache_path.encode() if cache_path else None)
+        rep = SjAutotuneReport()
+        check(self.lib.sj_autotune(self.h, C.byref(plan), C.byref(opts), C.byref(rep), stream))
+        q = dict(query)
+        q["bf_bits_per_key"] = plan.bf_bits_per_key
+        q["bf_hashes"] = plan.bf_hashes
+        q["order"] = [plan.order[i] for i in range(len(query["dims"]))]
+        tune = {f: getattr(plan.tune, f) for f, _ in SjTuning._fields_}
+        return q, tune, rep
 
     def prepare(self, query, cols, fact_rows, tune=None) -> "Query":
         plan, keep = fill_plan(query, cols, fact_rows, tune)

@@ -213,6 +213,39 @@ sj_status sj_ssb_q33_run_noalloc(int device,
                                  sj_group_row* out, int64_t cap, int64_t* n_out, void* stream);
 const char* sj_noalloc_last_error(void);
 
+/* ---- autotuner ----------------------------------------------------------
+ * Chooses the probe's launch geometry (threads per CTA, rows per lane, rows per
+ * stage, stage count) and, when asked, the filter kind (direct bitmap or
+ * blocked Bloom filter with 4/8/16 bits per key and 1..4 bits set per key) and
+ * the join order, by timing candidates on the plan's own columns (coordinate
+ * descent: filter, then geometry, then order).  Every candidate's groups must
+ * equal the first candidate's, bit for bit.  With a cache file, the winner is
+ * stored under a signature of the plan (table sizes, grouping, and each
+ * dimension's selectivity rounded to a power of 2) and later plans with the
+ * same signature take it without a search.  No counterpart in the reference,
+ * whose geometry is fixed at compile time (src/ssb-jo/q33/0-lip.cu:46-52). */
+typedef struct sj_autotune_opts {
+  int32_t reps;            /* timed probes per candidate (0 = 5) */
+  int32_t tune_filter;     /* 1: also choose bf_bits_per_key / bf_hashes */
+  int32_t tune_order;      /* 0: keep the plan's order, 1: most selective first, 2: time every order */
+  int32_t verify;          /* 1: compare every candidate's groups with the first's */
+  const char* cache_path;  /* tuning cache file, or NULL */
+} sj_autotune_opts;
+
+typedef struct sj_autotune_report {
+  int32_t candidates;      /* plans timed */
+  int32_t cache_hit;       /* 1: taken from the cache, nothing timed */
+  int32_t mismatches;      /* candidates whose groups differed (0 unless the engine is wrong) */
+  float default_ms;        /* probe time of the plan as given */
+  float best_ms;           /* probe time of the chosen plan */
+  double selectivity[SJ_MAX_DIMS];  /* qualifying fraction of each dimension's rows */
+} sj_autotune_report;
+
+/* plan is in/out: on success its tune, bf_bits_per_key, bf_hashes and order
+ * hold the choice.  Device columns only. */
+sj_status sj_autotune(sj_engine* e, sj_plan* plan, const sj_autotune_opts* opts, sj_autotune_report* report,
+                      void* stream);
+
 /* ---- Bloom filter unit interface (tests; the reference's src/ops/bloom.cu) -- */
 /* Build a filter over keys[flags != 0] and probe probe_keys; out_flags[i] = 1 if
  * probe_keys[i] may be present.  All pointers are device pointers.

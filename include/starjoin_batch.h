@@ -95,7 +95,7 @@ typedef struct sjb_limits {
   int64_t filter_cache_bytes;        /* device bytes for cached filter bitmaps; 0 = 1 GiB */
   int32_t use_graph;                 /* 1: replay the batch pipeline as one CUDA graph */
   int32_t cache_filters;             /* 1: keep filter bitmaps across batches, keyed by predicate */
-  int32_t threads;                   /* probe CTA size (0 = 512) */
+  int32_t threads;                   /* probe CTA size: 256, 512 or 1024 (0 = 1024) */
   int32_t smem_group_entries;        /* per-CTA shared-memory group partials (0 = 6144) */
 } sjb_limits;
 
@@ -148,6 +148,8 @@ typedef struct sjs_stats {
   uint64_t filters_built, filters_cached;
   uint64_t peak_active;
   double busy_s;                     /* wall time the loop spent with work */
+  double admit_s;                    /* ... of which admitting (filter builds, layout) */
+  double scan_s;                     /* ... of which scan steps (probe, results) */
 } sjs_stats;
 
 sj_status sjs_server_create(sj_engine* eng, const sjb_schema* schema, const sjs_config* cfg, sjs_server** out);
