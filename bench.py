@@ -413,10 +413,21 @@ def main():
     ap.add_argument("--shared", choices=["batch", "serve"],
                     help="run only the batched or the serving measurement (--rows sets the fact table)")
     ap.add_argument("--batches", type=int, default=6, help="timed batches of the batched measurement")
+    ap.add_argument("--sweep4", type=int, nargs="?", const=256, default=None,
+                    help="run only the 4-dimension selectivity x filter sweep (optionally the first N of its "
+                         "256 selectivity settings)")
     args = ap.parse_args()
     FACT_ROWS = args.rows
     args.warmup = max(3, args.warmup)
-    if args.shared:
+    if args.sweep4 is not None:
+        import itertools
+        import starjoin as sj
+        import sweep_bench
+        eng = sj.Engine(0)
+        settings = list(itertools.product(sweep_bench.SELS, repeat=4))[: args.sweep4]
+        print(json.dumps({"sweep4": sweep_bench.sweep4(eng, settings=settings)}), flush=True)
+        eng.close()
+    elif args.shared:
         run_shared(args)
     elif args.impl == "reference":
         run_reference(args)
