@@ -413,6 +413,9 @@ def main():
     ap.add_argument("--shared", choices=["batch", "serve"],
                     help="run only the batched or the serving measurement (--rows sets the fact table)")
     ap.add_argument("--batches", type=int, default=6, help="timed batches of the batched measurement")
+    ap.add_argument("--rates", default="200,2000",
+                    help="Poisson arrival rates (queries/s) of the serving measurement, comma-separated; "
+                         "'none' measures saturation only")
     ap.add_argument("--sweep4", type=int, nargs="?", const=256, default=None,
                     help="run only the 4-dimension selectivity x filter sweep (optionally the first N of its "
                          "256 selectivity settings)")
@@ -449,7 +452,8 @@ def run_shared(args):
         schema = dict(sb.SERVE_SCHEMA)
         if args.rows != 120_000_000:
             schema["fact_rows"] = args.rows
-        out = {"serving": sb.serving(eng, schema=schema)}
+        rates = () if args.rates == "none" else tuple(float(x) for x in args.rates.split(",") if x)
+        out = {"serving": sb.serving(eng, schema=schema, rates=rates)}
     print(json.dumps(out), flush=True)
     eng.close()
 

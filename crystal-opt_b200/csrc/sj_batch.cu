@@ -79,96 +79,149 @@ __global__ void __launch_bounds__(256) sjb_zero_jobs_kernel(const SjbBatchDesc* 
     reinterpret_cast<uint32_t*>(J.stats)[threadIdx.x] = 0u;
 }
 
-__global__ void __launch_bounds__(256) sjb_build_kernel(const __grid_constant__ SjbSchemaRt S,
-                                                        const SjbBatchDesc* __restrict__ D) {
-  const uint32_t j = blockIdx.y;
-  if (j >= D->n_jobs) return;
-  const SjbJob J = D->jobs[j];
-  const SjbDimRt& R = S.dim[J.dim];
-  const uint32_t* inb = J.in_index >= 0 ? D->in_bits[J.in_index] : nullptr;
-  const uint32_t lane = threadIdx.x & 31u;
-  uint32_t cnt = 0;
-  uint32_t umax[SJB_MAX_ATTRS] = {0, 0, 0, 0}, nmin[SJB_MAX_ATTRS] = {0, 0, 0, 0};
+// One pass per dimension serves all of that dimension's jobs: each row's key
+// and attributes are read once, then every job's predicate is evaluated on them
+// (blockIdx.y = dimension).  Per job and warp: one ballot, one atomicOr per
+// distinct bitmap word, and the statistics only when some row qualified, kept
+// in shared memory and flushed once per block.
+constexpr uint32_t kBuildThreads = 256;
+
+__global__ void __launch_bounds__(kBuildThreads) sjb_build_kernel(const __grid_constant__ SjbSchemaRt S,
+                                                                  const SjbBatchDesc* __restrict__ D) {
+  __shared__ SjbJob s_job[kBMaxJobs];
+  __shared__ uint32_t s_cnt[kBMaxJobs];
+  __shared__ uint32_t s_umax[kBMaxJobs][SJB_MAX_ATTRS], s_nmin[kBMaxJobs][SJB_MAX_ATTRS];
+  __shared__ uint32_t s_nj, s_warp_base[kBuildThreads / 32];
+  const uint32_t d = blockIdx.y;
+  if (d >= S.n_dims) return;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
+  const uint32_t nj_all = min(D->n_jobs, (uint32_t)kBMaxJobs);
+  // this dimension's jobs, compacted in job order
+  const bool mine = tid < nj_all && D->jobs[tid].dim == d;
+  const uint32_t bal = __ballot_sync(kFull, mine);
+  if (lane == 0) s_warp_base[wid] = __popc(bal);
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t run = 0;
+    for (uint32_t w = 0; w < kBuildThreads / 32; ++w) {
+      const uint32_t c = s_warp_base[w];
+      s_warp_base[w] = run;
+      run += c;
+    }
+    s_nj = run;
+  }
+  __syncthreads();
+  if (mine) {
+    const uint32_t k = s_warp_base[wid] + __popc(bal & ((1u << lane) - 1u));
+    s_job[k] = D->jobs[tid];
+    s_cnt[k] = 0;
+    for (uint32_t a = 0; a < SJB_MAX_ATTRS; ++a) s_umax[k][a] = s_nmin[k][a] = 0;
+  }
+  __syncthreads();
+  const uint32_t nj = s_nj;
+  if (nj == 0) return;
+  const SjbDimRt& R = S.dim[d];
+  const uint32_t na = R.n_attrs;
   // the loop bound is uniform across the warp, so full-warp collectives are safe inside
-  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < R.rows; i0 += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = i0 + threadIdx.x;
-    bool ok = i < R.rows;
-    const int32_t key = ok ? R.key[i] : 0;
-    ok = ok && key != 0;  // CAS(slot, 0, 0) never claims a slot (crystal/join.cuh:270)
-    if (ok && J.kind != SJ_PRED_ALL) {
-      const int32_t a = R.attr[J.attr][i];
-      if (J.kind == SJ_PRED_RANGE)
-        ok = a >= J.lo && a <= J.hi;
-      else
-        ok = (uint32_t)a < (uint32_t)SJ_MAX_IN_CODES && ((inb[(uint32_t)a >> 5] >> ((uint32_t)a & 31u)) & 1u);
-    }
-    const uint32_t s = ok ? slot_of(key, R.key_min, R.len, R.fastmod_m) : 0u;
-    const uint32_t w = s >> 5, bit = 1u << (s & 31u);
-    uint32_t pend = __ballot_sync(kFull, ok);
-    while (pend) {  // one atomicOr per distinct bitmap word in the warp
-      const uint32_t leader = __ffs(pend) - 1u;
-      const uint32_t lw = __shfl_sync(kFull, w, leader);
-      const bool mine = ((pend >> lane) & 1u) && w == lw;
-      const uint32_t bits = __reduce_or_sync(kFull, mine ? bit : 0u);
-      if (lane == leader) atomicOr(J.bitmap + lw, bits);
-      pend &= ~__ballot_sync(kFull, mine);
-    }
-    if (ok) {
-      ++cnt;
+  for (int64_t i0 = (int64_t)blockIdx.x * kBuildThreads; i0 < R.rows; i0 += (int64_t)gridDim.x * kBuildThreads) {
+    const int64_t i = i0 + tid;
+    const bool in = i < R.rows;
+    const int32_t key = in ? R.key[i] : 0;
+    int32_t av[SJB_MAX_ATTRS];
+#pragma unroll
+    for (uint32_t a = 0; a < SJB_MAX_ATTRS; ++a) av[a] = (in && a < na) ? R.attr[a][i] : 0;
+    const bool live = in && key != 0;  // CAS(slot, 0, 0) never claims a slot (crystal/join.cuh:270)
+    const uint32_t s = live ? slot_of(key, R.key_min, R.len, R.fastmod_m) : 0u;
+    const uint32_t wd = s >> 5, bit = 1u << (s & 31u);
+    uint32_t uv[SJB_MAX_ATTRS];
+#pragma unroll
+    for (uint32_t a = 0; a < SJB_MAX_ATTRS; ++a) uv[a] = (uint32_t)av[a] ^ 0x80000000u;
+    for (uint32_t k = 0; k < nj; ++k) {
+      const SjbJob& J = s_job[k];
+      bool ok = live;
+      if (ok && J.kind != SJ_PRED_ALL) {
+        int32_t a = av[0];
+#pragma unroll
+        for (uint32_t x = 1; x < SJB_MAX_ATTRS; ++x) a = (uint32_t)J.attr == x ? av[x] : a;
+        if (J.kind == SJ_PRED_RANGE)
+          ok = a >= J.lo && a <= J.hi;
+        else
+          ok = (uint32_t)a < (uint32_t)SJ_MAX_IN_CODES &&
+               ((D->in_bits[J.in_index][(uint32_t)a >> 5] >> ((uint32_t)a & 31u)) & 1u);
+      }
+      uint32_t pend = __ballot_sync(kFull, ok);
+      if (!pend) continue;  // warp-uniform
+      const uint32_t n_ok = __popc(pend);
+      while (pend) {  // one atomicOr per distinct bitmap word in the warp
+        const uint32_t leader = __ffs(pend) - 1u;
+        const uint32_t lw = __shfl_sync(kFull, wd, leader);
+        const bool hit = ((pend >> lane) & 1u) && wd == lw;
+        const uint32_t bits = __reduce_or_sync(kFull, hit ? bit : 0u);
+        if (lane == leader) atomicOr(J.bitmap + lw, bits);
+        pend &= ~__ballot_sync(kFull, hit);
+      }
+      if (lane == 0) atomicAdd(&s_cnt[k], n_ok);
 #pragma unroll
       for (uint32_t a = 0; a < SJB_MAX_ATTRS; ++a) {
-        if (a < R.n_attrs) {
-          const uint32_t u = (uint32_t)R.attr[a][i] ^ 0x80000000u;
-          umax[a] = max(umax[a], u);
-          nmin[a] = max(nmin[a], ~u);
+        if (a < na) {
+          const uint32_t mx = __reduce_max_sync(kFull, ok ? uv[a] : 0u);
+          const uint32_t mn = __reduce_max_sync(kFull, ok ? ~uv[a] : 0u);
+          if (lane == 0) {
+            atomicMax(&s_umax[k][a], mx);
+            atomicMax(&s_nmin[k][a], mn);
+          }
         }
       }
     }
   }
-  cnt = __reduce_add_sync(kFull, cnt);
-#pragma unroll
-  for (uint32_t a = 0; a < SJB_MAX_ATTRS; ++a) {
-    umax[a] = __reduce_max_sync(kFull, umax[a]);
-    nmin[a] = __reduce_max_sync(kFull, nmin[a]);
-  }
-  if (lane == 0 && cnt) {
-    atomicAdd(&J.stats->count, cnt);
-    for (uint32_t a = 0; a < R.n_attrs; ++a) {
-      atomicMax(&J.stats->umax[a], umax[a]);
-      atomicMax(&J.stats->nmin[a], nmin[a]);
+  __syncthreads();
+  for (uint32_t k = tid; k < nj; k += kBuildThreads) {
+    if (!s_cnt[k]) continue;
+    SjbEntryStats* st = s_job[k].stats;
+    atomicAdd(&st->count, s_cnt[k]);
+    for (uint32_t a = 0; a < na; ++a) {
+      atomicMax(&st->umax[a], s_umax[k][a]);
+      atomicMax(&st->nmin[a], s_nmin[k][a]);
     }
   }
 }
 
 cudaError_t sjb_launch_build(const SjbSchemaRt& S, const SjbBatchDesc* desc, uint32_t max_jobs,
                              uint32_t jobs_hint, int sm_count, cudaStream_t st) {
+  (void)jobs_hint;
   if (max_jobs == 0) return cudaSuccess;
   uint64_t max_len = 1, max_rows = 1;
   for (uint32_t d = 0; d < S.n_dims; ++d) {
     max_len = std::max<uint64_t>(max_len, S.dim[d].len);
     max_rows = std::max<uint64_t>(max_rows, (uint64_t)S.dim[d].rows);
   }
-  // enough blocks for the largest dimension, fewer per job when many jobs share the GPU
-  const uint32_t per_job = (uint32_t)std::max<uint64_t>(
-      1, std::min<uint64_t>((max_rows + 255) / 256,
-                            (uint64_t)std::max(1, sm_count * 8 / (int)std::max(1u, std::min(jobs_hint, 64u)))));
   const uint32_t zblocks = (uint32_t)std::min<uint64_t>((max_len / 32 + 256) / 256, 64);
   sjb_zero_jobs_kernel<<<dim3(zblocks, max_jobs), 256, 0, st>>>(desc);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  sjb_build_kernel<<<dim3(per_job, max_jobs), 256, 0, st>>>(S, desc);
+  // enough blocks to fill the GPU on the largest dimension
+  const uint32_t bx = (uint32_t)std::max<uint64_t>(
+      1, std::min<uint64_t>((max_rows + kBuildThreads - 1) / kBuildThreads, (uint64_t)sm_count * 4));
+  sjb_build_kernel<<<dim3(bx, S.n_dims), kBuildThreads, 0, st>>>(S, desc);
   return cudaGetLastError();
 }
 
 // --------------------------------------------------------------- layout ----
-// One thread per query computes its group layout; thread 0 then assigns
-// accumulator ranges, shared-memory partials and the lookup order.
+// One thread per query slot (two warps).  Each thread computes its query's group
+// layout; accumulator offsets are a warp scan of the spans, the dimension use
+// masks are ballots, and the shared-memory partials go to the smallest spans
+// first (each candidate's offset is the sum of the spans ranked before it).
 __global__ void __launch_bounds__(kBq) sjb_layout_kernel(const __grid_constant__ SjbSchemaRt S,
                                                          const SjbBatchDesc* __restrict__ D,
                                                          SjbStep* __restrict__ out, SjbCounters* ctr) {
   __shared__ SjbStep st;
   __shared__ uint32_t s_err;
-  const uint32_t q = threadIdx.x;
+  __shared__ unsigned long long s_wsum[2], s_wact[2], s_wuse[2][SJ_MAX_DIMS];
+  __shared__ float s_wcost[2][SJ_MAX_DIMS];
+  __shared__ long long s_wlo[2], s_whi[2];
+  __shared__ uint32_t s_span[kBq], s_smax[2];
+  __shared__ uint8_t s_pos[SJ_MAX_DIMS];
+  const uint32_t q = threadIdx.x, lane = q & 31u, wp = q >> 5;
   if (q == 0) s_err = 0;
   __syncthreads();
   SjbSlot& sl = st.slot[q];
@@ -192,30 +245,87 @@ __global__ void __launch_bounds__(kBq) sjb_layout_kernel(const __grid_constant__
     sl.b = Q.b;
     sl.e = Q.e;
   }
+  const bool act = q < D->n_queries && sl.span > 0 && sl.e > sl.b;
+  // accumulator offsets: exclusive scan of the active spans in slot order
+  unsigned long long incl = act ? sl.span : 0ull;
+  for (uint32_t off = 1; off < 32; off <<= 1) {
+    const unsigned long long v = __shfl_up_sync(kFull, incl, off);
+    if (lane >= off) incl += v;
+  }
+  const unsigned long long wtot = __shfl_sync(kFull, incl, 31);
+  const uint32_t ab = __ballot_sync(kFull, act);
+  float cost[SJ_MAX_DIMS];
+  uint32_t ub[SJ_MAX_DIMS];
+  for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) {
+    const bool u = act && st.bm[q][d] != nullptr;
+    ub[d] = __ballot_sync(kFull, u);
+    float c = act ? (u ? st.sel[q][d] : 1.f) : 0.f;
+    for (uint32_t off = 16; off; off >>= 1) c += __shfl_xor_sync(kFull, c, off);
+    cost[d] = c;
+  }
+  long long lo = act ? sl.b : LLONG_MAX, hi = act ? sl.e : 0;
+  for (uint32_t off = 16; off; off >>= 1) {
+    lo = min(lo, __shfl_xor_sync(kFull, lo, off));
+    hi = max(hi, __shfl_xor_sync(kFull, hi, off));
+  }
+  if (lane == 0) {
+    s_wsum[wp] = wtot;
+    s_wact[wp] = ab;
+    s_wlo[wp] = lo;
+    s_whi[wp] = hi;
+    for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) {
+      s_wuse[wp][d] = ub[d];
+      s_wcost[wp][d] = cost[d];
+    }
+  }
   __syncthreads();
+  const unsigned long long total = s_wsum[0] + s_wsum[1];
+  const bool over = total > D->group_capacity;
+  sl.group_base = incl - (act ? sl.span : 0ull) + (wp ? s_wsum[0] : 0ull);
+  const uint64_t active = over ? 0ull : (s_wact[0] | (s_wact[1] << 32));
+  const bool a2 = (active >> q) & 1ull;
   if (q == 0) {
-    uint64_t active = 0, base = 0;
-    int64_t lo = INT64_MAX, hi = 0;
-    for (int i = 0; i < kBq; ++i) {
-      SjbSlot& s = st.slot[i];
-      if (!(i < (int)D->n_queries && s.span > 0 && s.e > s.b)) continue;
-      s.group_base = base;
-      base += s.span;
-      active |= 1ull << i;
-      lo = min(lo, s.b);
-      hi = max(hi, s.e);
-    }
-    if (base > D->group_capacity) {
-      s_err |= kBErrGroupCapacity;
-      active = 0;
-    }
+    if (over) s_err |= kBErrGroupCapacity;
     st.active = active;
-    st.seg_b = active ? lo : 0;
-    st.seg_e = active ? hi : 0;
+    st.seg_b = active ? min(s_wlo[0], s_wlo[1]) : 0;
+    st.seg_e = active ? max(s_whi[0], s_whi[1]) : 0;
+    st.n_dims = S.n_dims;
+    float c[SJ_MAX_DIMS];
+    for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) {
+      st.use[d] = over ? 0ull : (s_wuse[0][d] | (s_wuse[1][d] << 32));
+      c[d] = s_wcost[0][d] + s_wcost[1][d];
+      st.order[d] = d;
+    }
+    for (uint32_t a = 1; a < S.n_dims; ++a)  // fewest expected surviving candidates first
+      for (uint32_t b = a; b > 0 && c[st.order[b]] < c[st.order[b - 1]]; --b) {
+        const uint32_t t = st.order[b];
+        st.order[b] = st.order[b - 1];
+        st.order[b - 1] = t;
+      }
+    for (uint32_t k = 0; k < S.n_dims; ++k) s_pos[st.order[k]] = (uint8_t)k;
     st.error = s_err;
-    sjb_step_layout(st, S.n_dims, D->smem_capacity);
     if (s_err) atomicOr(&ctr->error, s_err);
   }
+  const bool cand = a2 && sl.span <= 2048u;
+  s_span[q] = cand ? sl.span : 0u;
+  __syncthreads();
+  for (int g = 0; g < sl.n_g; ++g) sl.gpos[g] = s_pos[sl.gd[g]];
+  uint32_t end = 0;
+  if (cand) {  // offset = spans of the candidates ranked before this one (smaller span, then lower slot)
+    uint32_t off = 0;
+    for (uint32_t r = 0; r < (uint32_t)kBq; ++r) {
+      const uint32_t sr = s_span[r];
+      if (sr && (sr < sl.span || (sr == sl.span && r < q))) off += sr;
+    }
+    if (off + sl.span <= D->smem_capacity) {
+      sl.smem_off = (int32_t)off;
+      end = off + sl.span;
+    }
+  }
+  for (uint32_t o = 16; o; o >>= 1) end = max(end, __shfl_xor_sync(kFull, end, o));
+  if (lane == 0) s_smax[wp] = end;
+  __syncthreads();
+  if (q == 0) st.smem_entries = max(s_smax[0], s_smax[1]);
   __syncthreads();
   const uint32_t* src = reinterpret_cast<const uint32_t*>(&st);
   uint32_t* dst = reinterpret_cast<uint32_t*>(out);
@@ -536,7 +646,9 @@ __global__ void __launch_bounds__(256) sjb_finalize_kernel(const SjbStep* __rest
                                                            uint64_t cap, SjbCounters* ctr,
                                                            const int32_t* __restrict__ slot_query) {
   const uint32_t q = blockIdx.y;
-  if (!((G->active & mask) >> q & 1ull)) return;
+  // slot_query given: `mask` alone names the slots (serving); else the step's active slots
+  const uint64_t sel = slot_query ? mask : (G->active & mask);
+  if (!((sel >> q) & 1ull)) return;
   const SjbSlot& s = G->slot[q];
   const uint32_t lane = threadIdx.x & 31u;
   const int32_t qid = slot_query ? slot_query[q] : (int32_t)q;

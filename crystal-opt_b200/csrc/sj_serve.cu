@@ -82,13 +82,27 @@ struct sjs_server {
   uint8_t* arena = nullptr;
   SjbEntryStats* stats_d = nullptr;
   int32_t* slot_query_d = nullptr;
-  // pinned
-  SjbStep* step_h[2] = {nullptr, nullptr};
+  // pinned (double-buffered per step: [buffer][0 = composition, 1 = probe])
+  SjbStep* step_h[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   SjbBatchDesc* desc_h = nullptr;
   SjbCounters* ctr_h = nullptr;
   SjbEntryStats* stats_h = nullptr;
   int32_t* slot_query_h = nullptr;
-  cudaStream_t st = nullptr;
+  sjb_row* rows_h[2] = {nullptr, nullptr};
+  cudaStream_t st = nullptr;   // scan steps
+  cudaStream_t stb = nullptr;  // admission: filter builds, accumulator clears
+  cudaEvent_t ev_probe[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  cudaEvent_t ev_done[2] = {nullptr, nullptr};
+  cudaEvent_t ev_admitted = nullptr;
+  struct StepRec {
+    bool valid = false;
+    bool probed = false;
+    uint64_t fin = 0;          // slots whose groups this step reads back
+    uint64_t bound = 0;        // result rows copied back (sum of their spans)
+  } rec[2];
+  int next_buf = 0;            // buffer of the next step launch
+  uint64_t fin_queued = 0;     // finished slots whose read-back is enqueued
+  int64_t next_pos = 0;        // scan position after the last launched step
   FilterCache cache;
   RangeAlloc groups;
   // loop state
@@ -100,7 +114,6 @@ struct sjs_server {
   uint64_t next_ticket = 1;
   bool stop = false;
   Slot slots[kBq];
-  int64_t pos = 0;
   bool masks_dirty = true;
   sjs_stats stats{};
   std::string loop_error;
@@ -262,19 +275,19 @@ bool admit(sjs_server* s) {
   if (D.n_jobs) {
     // upload the header and the jobs in use, then the IN-code bitmaps in use
     const size_t head = offsetof(SjbBatchDesc, jobs) + sizeof(SjbJob) * D.n_jobs;
-    if (cudaMemcpyAsync(s->desc_d, s->desc_h, head, cudaMemcpyHostToDevice, s->st) != cudaSuccess) return false;
+    if (cudaMemcpyAsync(s->desc_d, s->desc_h, head, cudaMemcpyHostToDevice, s->stb) != cudaSuccess) return false;
     if (n_in && cudaMemcpyAsync(s->desc_d->in_bits, s->desc_h->in_bits, sizeof(uint32_t) * kBInWords * n_in,
-                                cudaMemcpyHostToDevice, s->st) != cudaSuccess)
+                                cudaMemcpyHostToDevice, s->stb) != cudaSuccess)
       return false;
-    if (sjb_launch_build(s->S.rt, s->desc_d, D.n_jobs, D.n_jobs, s->eng->sm_count, s->st) != cudaSuccess)
+    if (sjb_launch_build(s->S.rt, s->desc_d, D.n_jobs, D.n_jobs, s->eng->sm_count, s->stb) != cudaSuccess)
       return false;
     // one read-back of the statistics records (indexed by entry id)
     uint32_t hi = 0;
     for (int id : new_ids) hi = std::max(hi, s->cache.at(id).stats_idx + 1);
-    if (cudaMemcpyAsync(s->stats_h, s->stats_d, sizeof(SjbEntryStats) * hi, cudaMemcpyDeviceToHost, s->st) !=
+    if (cudaMemcpyAsync(s->stats_h, s->stats_d, sizeof(SjbEntryStats) * hi, cudaMemcpyDeviceToHost, s->stb) !=
         cudaSuccess)
       return false;
-    if (cudaStreamSynchronize(s->st) != cudaSuccess) return false;
+    if (cudaStreamSynchronize(s->stb) != cudaSuccess) return false;
     for (size_t i = 0; i < new_ids.size(); ++i) {
       FilterEntry& e = s->cache.at(new_ids[i]);
       e.host = s->stats_h[e.stats_idx];
@@ -352,16 +365,19 @@ bool admit(sjs_server* s) {
     sl.group_span = span;
     sl.lay = lay;
     sl.lay.group_base = off;
-    // the scan is at `pos`: rows [pos, e) come first, then [b, pos) after the wrap
-    const int64_t b = bq.b, e = bq.e, p = s->pos;
+    // the next step starts at next_pos: rows [next_pos, e) come first, then [b, next_pos) after the wrap
+    const int64_t b = bq.b, e = bq.e, p = s->next_pos;
     if (p > b && p < e) {
       sl.remaining = {{p, e}, {b, p}};
     } else {
       sl.remaining = {{b, e}};
     }
-    if (cudaMemsetAsync(s->acc + off, 0, sizeof(SjbAcc) * span, s->st) != cudaSuccess) return false;
+    if (cudaMemsetAsync(s->acc + off, 0, sizeof(SjbAcc) * span, s->stb) != cudaSuccess) return false;
     s->masks_dirty = true;
   }
+  // the next scan step waits for the accumulator clears
+  if (cudaEventRecord(s->ev_admitted, s->stb) != cudaSuccess) return false;
+  if (cudaStreamWaitEvent(s->st, s->ev_admitted, 0) != cudaSuccess) return false;
   uint64_t act = 0;
   for (const Slot& sl : s->slots) act += sl.used;
   std::lock_guard<std::mutex> g(s->mu);
@@ -386,8 +402,9 @@ void fill_step(sjs_server* s, SjbStep& st, bool all, int64_t seg_b, int64_t seg_
       st.sel[q][d] = sl.sel[d];
     }
     if (!sl.used) continue;
-    if (all) {
-      active |= 1ull << q;
+    if (all) {  // slot words for the slots still scanning
+      if (!sl.remaining.empty()) active |= 1ull << q;
+      else for (int d = 0; d < SJ_MAX_DIMS; ++d) st.bm[q][d] = nullptr;
       continue;
     }
     const Interval iv = take(sl, seg_b, seg_e);
@@ -401,86 +418,105 @@ void fill_step(sjs_server* s, SjbStep& st, bool all, int64_t seg_b, int64_t seg_
   sjb_step_layout(st, s->S.rt.n_dims, 6144u);
 }
 
-bool run_step(sjs_server* s) {
+// Launch the next scan step into buffer set `b` (asynchronous): recompose the
+// slot words if the set of queries changed, probe the next segment some query
+// still needs, and queue the read-back of every query that step finishes.
+// Which queries a step finishes is known when it is planned, so their group
+// compaction and copies go into the stream right behind the probe; the host
+// collects them (complete_step) while the next step already runs.
+bool launch_step(sjs_server* s, bool* launched) {
+  *launched = false;
+  const int b = s->next_buf;
   const int64_t n = s->S.rt.fact_rows;
   if (s->masks_dirty) {
-    fill_step(s, *s->step_h[0], true, 0, 0);
-    if (cudaMemcpyAsync(s->step_d, s->step_h[0], sizeof(SjbStep), cudaMemcpyHostToDevice, s->st) != cudaSuccess)
+    fill_step(s, *s->step_h[b][0], true, 0, 0);
+    if (cudaMemcpyAsync(s->step_d, s->step_h[b][0], sizeof(SjbStep), cudaMemcpyHostToDevice, s->st) != cudaSuccess)
       return false;
     if (sjb_launch_compose(s->S.rt, s->step_d, s->eng->sm_count, s->st) != cudaSuccess) return false;
     s->masks_dirty = false;
   }
-  const int64_t p = next_needed(s, s->pos, n);
-  if (p < 0) return true;
-  const int64_t seg_b = p, seg_e = std::min<int64_t>(n, p + s->step_rows);
-  SjbStep& st = *s->step_h[1];
-  fill_step(s, st, false, seg_b, seg_e);
-  if (cudaMemcpyAsync(s->step_d, s->step_h[1], sizeof(SjbStep), cudaMemcpyHostToDevice, s->st) != cudaSuccess)
-    return false;
-  if (cudaMemsetAsync(s->ctr_d, 0, sizeof(SjbCounters), s->st) != cudaSuccess) return false;
-  const uint32_t threads = s->cfg.limits.threads ? (uint32_t)s->cfg.limits.threads : 1024u;
-  if (sjb_launch_probe(s->S.rt, s->step_d, s->acc, s->ctr_d, threads, st.smem_entries, s->eng->sm_count, s->st) !=
-      cudaSuccess)
-    return false;
-  // coverage and finished queries
-  uint64_t fin = 0;
-  for (int q = 0; q < kBq; ++q) {
-    Slot& sl = s->slots[q];
-    if (!sl.used || !((st.active >> q) & 1ull)) continue;
-    cover(sl, {st.slot[q].b, st.slot[q].e});
-    if (sl.remaining.empty()) fin |= 1ull << q;
-  }
-  if (fin) {
-    for (int q = 0; q < kBq; ++q) s->slot_query_h[q] = q;
-    if (cudaMemcpyAsync(s->slot_query_d, s->slot_query_h, sizeof(int32_t) * kBq, cudaMemcpyHostToDevice, s->st) !=
+  SjbCounters* ctr = s->ctr_d + 2 * b;
+  const int64_t p = next_needed(s, s->next_pos, n);
+  bool probed = false;
+  if (p >= 0) {
+    const int64_t seg_b = p, seg_e = std::min<int64_t>(n, p + s->step_rows);
+    SjbStep& st = *s->step_h[b][1];
+    fill_step(s, st, false, seg_b, seg_e);
+    if (cudaMemcpyAsync(s->step_d, s->step_h[b][1], sizeof(SjbStep), cudaMemcpyHostToDevice, s->st) != cudaSuccess)
+      return false;
+    if (cudaMemsetAsync(ctr, 0, 2 * sizeof(SjbCounters), s->st) != cudaSuccess) return false;
+    const uint32_t threads = s->cfg.limits.threads ? (uint32_t)s->cfg.limits.threads : 1024u;
+    if (cudaEventRecord(s->ev_probe[b][0], s->st) != cudaSuccess) return false;
+    if (sjb_launch_probe(s->S.rt, s->step_d, s->acc, ctr, threads, st.smem_entries, s->eng->sm_count, s->st) !=
         cudaSuccess)
       return false;
-    // finalize the finished slots in groups whose spans fit the result buffer
-    uint64_t left = fin;
-    while (left) {
-      uint64_t part = 0, rows = 0;
-      for (int q = 0; q < kBq; ++q) {
-        if (!((left >> q) & 1ull)) continue;
-        const uint64_t sp = s->slots[q].group_span;
-        if (part && rows + sp > s->result_rows) continue;
-        part |= 1ull << q;
-        rows += sp;
-      }
-      left &= ~part;
-      if (cudaMemsetAsync(s->ctr_d + 1, 0, sizeof(SjbCounters), s->st) != cudaSuccess) return false;
-      // the finalize kernel reads slot spans and bases from step_d; keep its active set
-      if (sjb_launch_finalize(s->step_d, part, s->acc, s->rows_d, s->result_rows, s->ctr_d + 1, s->slot_query_d,
-                              s->eng->sm_count, s->st) != cudaSuccess)
-        return false;
-      if (cudaMemcpyAsync(s->ctr_h, s->ctr_d, 2 * sizeof(SjbCounters), cudaMemcpyDeviceToHost, s->st) !=
-          cudaSuccess)
-        return false;
-      if (cudaStreamSynchronize(s->st) != cudaSuccess) return false;
-      const uint64_t nrows = std::min<uint64_t>(s->ctr_h[1].out_rows, s->result_rows);
-      std::vector<sjb_row> all(nrows);
-      if (nrows && cudaMemcpy(all.data(), s->rows_d, sizeof(sjb_row) * nrows, cudaMemcpyDeviceToHost) != cudaSuccess)
-        return false;
-      std::vector<std::vector<sjb_row>> per(kBq);
-      for (const sjb_row& r : all) per[r.query].push_back(r);
-      for (int q = 0; q < kBq; ++q) {
-        if (!((part >> q) & 1ull)) continue;
-        for (sjb_row& r : per[q]) r.query = 0;
-        const uint64_t id = s->slots[q].ticket;
-        release_slot(s, q);
-        finish_ticket(s, id, SJ_OK, std::move(per[q]));
-      }
-    }
-  } else if (cudaMemcpyAsync(s->ctr_h, s->ctr_d, sizeof(SjbCounters), cudaMemcpyDeviceToHost, s->st) !=
-                 cudaSuccess ||
-             cudaStreamSynchronize(s->st) != cudaSuccess) {
-    return false;
+    if (cudaEventRecord(s->ev_probe[b][1], s->st) != cudaSuccess) return false;
+    for (int q = 0; q < kBq; ++q)
+      if ((st.active >> q) & 1ull) cover(s->slots[q], {st.slot[q].b, st.slot[q].e});
+    s->next_pos = seg_e >= n ? 0 : seg_e;
+    probed = true;
   }
-  {
+  // read back the finished slots (as many as the result buffer holds; the rest next time)
+  uint64_t fin = 0, bound = 0;
+  for (int q = 0; q < kBq; ++q) {
+    const Slot& sl = s->slots[q];
+    if (!sl.used || !sl.remaining.empty() || ((s->fin_queued >> q) & 1ull)) continue;
+    if (fin && bound + sl.group_span > s->result_rows) continue;
+    fin |= 1ull << q;
+    bound += sl.group_span;
+  }
+  if (!probed && !fin) return true;
+  if (fin) {
+    // step_d holds every used slot's layout (each upload copies them all)
+    if (!probed && cudaMemsetAsync(ctr + 1, 0, sizeof(SjbCounters), s->st) != cudaSuccess) return false;
+    if (sjb_launch_finalize(s->step_d, fin, s->acc, s->rows_d, s->result_rows, ctr + 1, s->slot_query_d,
+                            s->eng->sm_count, s->st) != cudaSuccess)
+      return false;
+    if (cudaMemcpyAsync(s->rows_h[b], s->rows_d, sizeof(sjb_row) * bound, cudaMemcpyDeviceToHost, s->st) !=
+        cudaSuccess)
+      return false;
+  }
+  if (cudaMemcpyAsync(s->ctr_h + 2 * b, ctr, 2 * sizeof(SjbCounters), cudaMemcpyDeviceToHost, s->st) != cudaSuccess)
+    return false;
+  if (cudaEventRecord(s->ev_done[b], s->st) != cudaSuccess) return false;
+  s->rec[b].valid = true;
+  s->rec[b].probed = probed;
+  s->rec[b].fin = fin;
+  s->rec[b].bound = bound;
+  s->fin_queued |= fin;
+  s->next_buf = b ^ 1;
+  *launched = true;
+  return true;
+}
+
+// Wait for the step in buffer set `b` and hand out the groups it read back.
+bool complete_step(sjs_server* s, int b) {
+  auto& r = s->rec[b];
+  if (!r.valid) return true;
+  if (cudaEventSynchronize(s->ev_done[b]) != cudaSuccess) return false;
+  r.valid = false;
+  const SjbCounters* c = s->ctr_h + 2 * b;
+  if (r.fin) {
+    const uint64_t nrows = std::min<uint64_t>(c[1].out_rows, r.bound);
+    std::vector<std::vector<sjb_row>> per(kBq);
+    for (uint64_t i = 0; i < nrows; ++i) per[s->rows_h[b][i].query].push_back(s->rows_h[b][i]);
+    for (int q = 0; q < kBq; ++q) {
+      if (!((r.fin >> q) & 1ull)) continue;
+      for (sjb_row& x : per[q]) x.query = 0;
+      const uint64_t id = s->slots[q].ticket;
+      release_slot(s, q);
+      s->fin_queued &= ~(1ull << q);
+      finish_ticket(s, id, SJ_OK, std::move(per[q]));
+    }
+  }
+  if (r.probed) {
+    float pms = 0.f;
+    if (cudaEventElapsedTime(&pms, s->ev_probe[b][0], s->ev_probe[b][1]) != cudaSuccess) pms = 0.f;
     std::lock_guard<std::mutex> g(s->mu);
-    s->stats.rows_scanned += s->ctr_h[0].rows_scanned;
+    s->stats.rows_scanned += c[0].rows_scanned;
+    s->stats.probe_device_s += pms * 1e-3;
     ++s->stats.steps;
   }
-  s->pos = seg_e >= n ? 0 : seg_e;
   return true;
 }
 
@@ -560,7 +596,7 @@ void loop(sjs_server* s) {
     for (const Slot& sl : s->slots) any_active |= sl.used;
     {
       std::unique_lock<std::mutex> g(s->mu);
-      if (!any_active)
+      if (!any_active && !s->rec[0].valid && !s->rec[1].valid)
         s->cv_work.wait(g, [&] { return s->stop || !s->pending.empty(); });
       if (s->stop) break;
     }
@@ -574,11 +610,16 @@ void loop(sjs_server* s) {
       }
       if (id) plain_one(s, id);
     } else {
+      // admission (filter builds on the second stream) overlaps the steps in flight;
+      // step k+1 is launched before step k's results are collected
       ok = admit(s);
       const double t1 = now_s();
       bool active = false;
       for (const Slot& sl : s->slots) active |= sl.used;
-      if (ok && active) ok = run_step(s);
+      bool launched = false;
+      if (ok && active) ok = launch_step(s, &launched);
+      if (ok && launched) ok = complete_step(s, s->next_buf);  // the older of the two buffer sets
+      else if (ok) ok = complete_step(s, 0) && complete_step(s, 1);  // nothing new: drain
       std::lock_guard<std::mutex> g(s->mu);
       s->stats.admit_s += t1 - t0;
       s->stats.scan_s += now_s() - t1;
@@ -607,6 +648,7 @@ void server_free(sjs_server* s) {
   if (!s) return;
   cudaSetDevice(s->eng->device);
   if (s->st) cudaStreamSynchronize(s->st);
+  if (s->stb) cudaStreamSynchronize(s->stb);
   cudaFree(s->acc);
   cudaFree(s->rows_d);
   cudaFree(s->ctr_d);
@@ -615,13 +657,21 @@ void server_free(sjs_server* s) {
   cudaFree(s->arena);
   cudaFree(s->stats_d);
   cudaFree(s->slot_query_d);
-  cudaFreeHost(s->step_h[0]);
-  cudaFreeHost(s->step_h[1]);
+  for (auto& pair : s->step_h)
+    for (auto& h : pair) cudaFreeHost(h);
   cudaFreeHost(s->desc_h);
   cudaFreeHost(s->ctr_h);
   cudaFreeHost(s->stats_h);
   cudaFreeHost(s->slot_query_h);
+  for (auto& h : s->rows_h) cudaFreeHost(h);
   if (s->st) cudaStreamDestroy(s->st);
+  if (s->stb) cudaStreamDestroy(s->stb);
+  if (s->ev_admitted) cudaEventDestroy(s->ev_admitted);
+  for (auto& pair : s->ev_probe)
+    for (auto& e : pair)
+      if (e) cudaEventDestroy(e);
+  for (auto& e : s->ev_done)
+    if (e) cudaEventDestroy(e);
   schema_release(s->S);
   delete s;
 }
@@ -669,25 +719,38 @@ extern "C" sj_status sjs_server_create(sj_engine* eng, const sjb_schema* schema,
   const uint32_t max_entries = 8192;
   step(cudaMalloc(&s->acc, sizeof(SjbAcc) * (size_t)groups));
   step(cudaMalloc(&s->rows_d, sizeof(sjb_row) * s->result_rows));
-  step(cudaMalloc(&s->ctr_d, 2 * sizeof(SjbCounters)));
+  step(cudaMalloc(&s->ctr_d, 4 * sizeof(SjbCounters)));
   step(cudaMalloc(&s->step_d, sizeof(SjbStep)));
   step(cudaMalloc(&s->desc_d, sizeof(SjbBatchDesc)));
   step(cudaMalloc(&s->arena, (size_t)fcache));
   step(cudaMalloc(&s->stats_d, sizeof(SjbEntryStats) * max_entries));
   step(cudaMalloc(&s->slot_query_d, sizeof(int32_t) * kBq));
-  step(cudaMallocHost(&s->step_h[0], sizeof(SjbStep)));
-  step(cudaMallocHost(&s->step_h[1], sizeof(SjbStep)));
+  for (auto& pair : s->step_h)
+    for (auto& h : pair) step(cudaMallocHost(&h, sizeof(SjbStep)));
   step(cudaMallocHost(&s->desc_h, sizeof(SjbBatchDesc)));
-  step(cudaMallocHost(&s->ctr_h, 2 * sizeof(SjbCounters)));
+  step(cudaMallocHost(&s->ctr_h, 4 * sizeof(SjbCounters)));
   step(cudaMallocHost(&s->stats_h, sizeof(SjbEntryStats) * max_entries));
   step(cudaMallocHost(&s->slot_query_h, sizeof(int32_t) * kBq));
   step(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  step(cudaStreamCreateWithFlags(&s->stb, cudaStreamNonBlocking));
+  step(cudaEventCreateWithFlags(&s->ev_admitted, cudaEventDisableTiming));
+  for (auto& h : s->rows_h) step(cudaMallocHost(&h, sizeof(sjb_row) * s->result_rows));
+  for (auto& pair : s->ev_probe)
+    for (auto& ev : pair) step(cudaEventCreate(&ev));
+  for (auto& ev : s->ev_done) step(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   if (e != cudaSuccess) {
     rc = cuda_fail(e, "sjs_server_create");
     server_free(s);
     return rc;
   }
   memset(s->desc_h, 0, sizeof(SjbBatchDesc));
+  for (int q = 0; q < kBq; ++q) s->slot_query_h[q] = q;
+  e = cudaMemcpy(s->slot_query_d, s->slot_query_h, sizeof(int32_t) * kBq, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    rc = cuda_fail(e, "sjs_server_create");
+    server_free(s);
+    return rc;
+  }
   s->cache.init(s->arena, (uint64_t)fcache, s->stats_d, max_entries);
   s->groups.reset((uint64_t)groups, 1);
   s->th = std::thread(loop, s);

@@ -195,7 +195,8 @@ def serving(eng: sj.Engine, rates=(200.0, 2000.0), seconds: float = 1.0, seed: i
                 r, rows = _poisson_run(srv, qs, float("inf"), seed)
                 st = srv.stats()
                 r.update({"steps": st.steps, "busy_s": st.busy_s, "admit_s": st.admit_s, "scan_s": st.scan_s,
-                          "peak_active": st.peak_active, "rows_scanned": st.rows_scanned})
+                          "probe_device_s": st.probe_device_s, "peak_active": st.peak_active,
+                          "rows_scanned": st.rows_scanned})
             finally:
                 srv.close()
             res["plain" if plain else "shared"] = r

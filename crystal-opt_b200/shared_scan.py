@@ -73,7 +73,8 @@ class SjsStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("finished", C.c_uint64),
                 ("rejected", C.c_uint64), ("steps", C.c_uint64), ("rows_scanned", C.c_uint64),
                 ("filters_built", C.c_uint64), ("filters_cached", C.c_uint64), ("peak_active", C.c_uint64),
-                ("busy_s", C.c_double), ("admit_s", C.c_double), ("scan_s", C.c_double)]
+                ("busy_s", C.c_double), ("admit_s", C.c_double), ("scan_s", C.c_double),
+                ("probe_device_s", C.c_double)]
 
 
 SYMBOLS = ["sjb_batch_create", "sjb_batch_destroy", "sjb_batch_run", "sjb_batch_get_stats",

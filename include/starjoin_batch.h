@@ -150,6 +150,7 @@ typedef struct sjs_stats {
   double busy_s;                     /* wall time the loop spent with work */
   double admit_s;                    /* ... of which admitting (filter builds, layout) */
   double scan_s;                     /* ... of which scan steps (probe, results) */
+  double probe_device_s;             /* device time of the shared-scan probes (CUDA events) */
 } sjs_stats;
 
 sj_status sjs_server_create(sj_engine* eng, const sjb_schema* schema, const sjs_config* cfg, sjs_server** out);
