@@ -80,6 +80,79 @@ __device__ void bitmap_prefix(const uint32_t* bm, uint32_t words, uint32_t* pre,
   __syncthreads();
 }
 
+// Expected filter-test cost per fact row of a LIP order: a test costs 1 when its
+// filter is in the probe's shared memory and kL2TestCost when it is read from
+// L2; a row reaches position p with the product of the earlier pass rates.
+constexpr float kL2TestCost = 4.f;
+
+// Starting LIP order and filter placement for the probe.  Filters take the
+// probe's shared memory in LIP order while they fit.  With adaptive LIP the
+// order is the cheapest one over all permutations, with each dimension's
+// qualifying fraction as its pass-rate estimate; otherwise the plan's order.
+__device__ void choose_start(const SjPlanRt& P, SjDesc* desc) {
+  const uint32_t n = P.n_dims;
+  uint32_t bytes[kMaxDims] = {0, 0, 0, 0};
+  float rate[kMaxDims] = {1.f, 1.f, 1.f, 1.f};
+  for (uint32_t d = 0; d < n; ++d) {
+    const SjDimRt& D = P.dim[d];
+    const uint32_t ins = desc->dim[d].n_inserted;
+    const uint32_t l2 = (D.bf_mode == kBfBlocked) ? bf_blocked_log2(ins, D.bf_bits_per_key, D.bf_max_log2)
+                                                  : D.bf_max_log2;
+    bytes[d] = (D.bf_mode == kBfDirect) ? max(8u, (1u << l2) / 8u) : (8u << l2);
+    rate[d] = ((float)ins + 1.f) / ((float)D.rows + 2.f);
+  }
+  auto place = [&](const uint32_t* ord, uint32_t* off, float* weight) {
+    uint32_t used = 0;
+    for (uint32_t p = 0; p < n; ++p) {
+      const uint32_t d = ord[p];
+      const bool fits = P.lip && used + bytes[d] <= P.bf_smem_budget;
+      off[d] = fits ? used : ~0u;
+      weight[d] = fits ? 1.f : kL2TestCost;
+      if (fits) used += (bytes[d] + 15u) & ~15u;
+    }
+  };
+  uint32_t best[kMaxDims] = {0, 1, 2, 3};
+  for (uint32_t p = 0; p < n; ++p) best[p] = P.order[p];
+  if (P.lip && P.adaptive && n > 1) {
+    uint32_t perm[kMaxDims] = {0, 1, 2, 3};
+    float best_cost = 3.4e38f;
+    for (;;) {
+      uint32_t off[kMaxDims];
+      float weight[kMaxDims];
+      place(perm, off, weight);
+      float cost = 0.f, live = 1.f;
+      for (uint32_t p = 0; p < n; ++p) {
+        cost += live * weight[perm[p]];
+        live *= rate[perm[p]];
+      }
+      if (cost < best_cost) {
+        best_cost = cost;
+        for (uint32_t p = 0; p < n; ++p) best[p] = perm[p];
+      }
+      int i = (int)n - 2;  // next permutation (lexicographic)
+      while (i >= 0 && perm[i] >= perm[i + 1]) --i;
+      if (i < 0) break;
+      int j = (int)n - 1;
+      while (perm[j] <= perm[i]) --j;
+      uint32_t t = perm[i];
+      perm[i] = perm[j];
+      perm[j] = t;
+      for (int a = i + 1, b = (int)n - 1; a < b; ++a, --b) {
+        t = perm[a];
+        perm[a] = perm[b];
+        perm[b] = t;
+      }
+    }
+  }
+  uint32_t off[kMaxDims] = {~0u, ~0u, ~0u, ~0u};
+  float weight[kMaxDims];
+  place(best, off, weight);
+  for (uint32_t d = 0; d < kMaxDims; ++d) {
+    desc->start_order[d] = d < n ? best[d] : 0u;
+    desc->bf_smem_off[d] = d < n ? off[d] : ~0u;
+  }
+}
+
 __global__ void __launch_bounds__(256) sj_dim_insert(const __grid_constant__ SjPlanRt P) {
   extern __shared__ uint32_t prefix[];  // payload-bitmap prefix popcounts
   __shared__ uint32_t s_total;
@@ -125,6 +198,7 @@ __global__ void __launch_bounds__(256) sj_dim_insert(const __grid_constant__ SjP
         groups *= (n ? n : 1u);
       }
       desc->n_groups = groups;
+      choose_start(P, desc);
     }
   }
 

@@ -350,6 +350,7 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
   rt.lip = p.lip ? 1u : 0u;
   rt.adaptive = p.adaptive ? 1u : 0u;
   rt.group_capacity = (uint32_t)groups;
+  rt.bf_smem_budget = q->geom.bf_smem_bytes;
   for (int i = 0; i < SJ_MAX_DIMS; ++i) rt.order[i] = (i < p.n_dims) ? (uint32_t)p.order[i] : 0u;
   q->in_bitmaps.assign(SJ_MAX_DIMS * (SJ_MAX_IN_CODES / 32), 0u);
   for (int d = 0; d < p.n_dims; ++d) {

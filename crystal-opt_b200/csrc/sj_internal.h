@@ -49,6 +49,8 @@ struct SjDimDev {
 // Per-query device descriptor (build writes, probe/finalize read, host fetches).
 struct SjDesc {
   SjDimDev dim[kMaxDims];
+  uint32_t start_order[kMaxDims];  // LIP order the probe starts with
+  uint32_t bf_smem_off[kMaxDims];  // filter offset in the probe's shared memory, ~0u: read from L2
   uint32_t n_groups;
   uint32_t error_flags;
   uint32_t groups_out;     // finalize: number of rows written
@@ -100,6 +102,7 @@ struct SjPlanRt {
   uint32_t adaptive;
   uint32_t order[kMaxDims];
   uint32_t group_capacity;    // allocated dense group slots
+  uint32_t bf_smem_budget;    // shared-memory bytes the probe holds filters in
 };
 
 // Launch geometry of the probe kernel.

@@ -216,6 +216,7 @@ extern "C" sj_status sj_ssb_q33_run_noalloc(int device, const int32_t* lo_orderd
   g.chunk_rows = 15360;
   g.stages = 2;
   g.bf_smem_bytes = 40u * 1024u;
+  rt.bf_smem_budget = g.bf_smem_bytes;
   g.group_smem_cap = 1024;
   g.q1_cap = 512;
   g.q2_cap = 64;

@@ -161,10 +161,15 @@ __device__ inline uint32_t make_steps(const SjPlanRt& P, const uint32_t* order, 
 }
 
 // Expected filter tests per row of an order under the observed pass rates.
-__device__ inline float order_cost(const float* rate, const uint32_t* order, uint32_t n) {
+// Expected filter-test cost per fact row of a LIP order: each test costs 1 when
+// its filter is in shared memory and kL2TestCost when it is read from L2, and
+// a row reaches position p with the product of the earlier pass rates.
+constexpr float kL2TestCost = 4.f;
+
+__device__ inline float order_cost(const float* rate, const float* weight, const uint32_t* order, uint32_t n) {
   float c = 0.f, live = 1.f;
   for (uint32_t p = 0; p < n; ++p) {
-    c += live;
+    c += live * weight[order[p]];
     live *= rate[order[p]];
   }
   return c;
@@ -465,23 +470,16 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
   // ---- setup (thread 0): plan steps, filter placement, mbarriers ----------
   if (tid == 0) {
     memset(&c, 0, sizeof(Ctl));
-    for (uint32_t d = 0; d < kMaxDims; ++d) c.order[0][d] = c.order[1][d] = P.order[d];
-    c.n_steps[0] = c.n_steps[1] = make_steps(P, P.order, c.steps[0]);
-    for (uint32_t p = 0; p < kMaxSteps; ++p) c.steps[1][p] = c.steps[0][p];
-    uint32_t used = 0;
-    for (uint32_t p = 0; p < P.n_dims; ++p) {
-      const uint32_t d = P.order[p];
-      const SjDimRt& D = P.dim[d];
-      const uint32_t l2 = desc->dim[d].bf_log2;
-      c.bf_log2[d] = l2;
-      const uint32_t bytes = (D.bf_mode == kBfDirect) ? max(8u, (1u << l2) / 8u) : (8u << l2);
-      if (P.lip && used + bytes <= G.bf_smem_bytes) {
-        c.bf_in_smem[d] = used;
-        used += align_up(bytes, 16);
-      } else {
-        c.bf_in_smem[d] = ~0u;
-      }
+    for (uint32_t d = 0; d < P.n_dims; ++d) c.bf_log2[d] = desc->dim[d].bf_log2;
+    // starting order and filter placement, chosen once per query by sj_dim_insert
+    uint32_t ord[kMaxDims];
+    for (uint32_t d = 0; d < kMaxDims; ++d) {
+      ord[d] = desc->start_order[d];
+      c.bf_in_smem[d] = desc->bf_smem_off[d];
     }
+    for (uint32_t d = 0; d < kMaxDims; ++d) c.order[0][d] = c.order[1][d] = (d < P.n_dims) ? ord[d] : 0u;
+    c.n_steps[0] = c.n_steps[1] = make_steps(P, ord, c.steps[0]);
+    for (uint32_t p = 0; p < kMaxSteps; ++p) c.steps[1][p] = c.steps[0][p];
     for (uint32_t d = 0; d < P.n_dims; ++d) c.group_stride[d] = desc->dim[d].group_stride;
     c.n_groups = desc->n_groups;
     c.groups_in_smem = c.n_groups <= G.group_smem_cap;
@@ -543,16 +541,20 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
             const float pa = (float)ld_volatile_u32(&c.passes[d]);
             rate[d] = (d < P.n_dims) ? (pa + 1.f) / (pr + 2.f) : 1.f;
           }
+          float weight[kMaxDims];
+          for (uint32_t d = 0; d < kMaxDims; ++d) weight[d] = (c.bf_in_smem[d] == ~0u) ? kL2TestCost : 1.f;
+          // candidate: sorted by observed pass rate (cheap on the issuing lane); taken
+          // when it cuts the placement-weighted cost by more than 10%
           uint32_t cand[kMaxDims];
           const uint32_t* cur = c.order[issue_ver];
           for (uint32_t d = 0; d < P.n_dims; ++d) cand[d] = cur[d];
-          for (uint32_t a = 1; a < P.n_dims; ++a)  // insertion sort by rate
+          for (uint32_t a = 1; a < P.n_dims; ++a)
             for (uint32_t b = a; b > 0 && rate[cand[b]] < rate[cand[b - 1]]; --b) {
               const uint32_t t = cand[b];
               cand[b] = cand[b - 1];
               cand[b - 1] = t;
             }
-          if (order_cost(rate, cand, P.n_dims) < 0.9f * order_cost(rate, cur, P.n_dims)) {
+          if (order_cost(rate, weight, cand, P.n_dims) < 0.9f * order_cost(rate, weight, cur, P.n_dims)) {
             const uint32_t nv = issue_ver ^ 1u;
             for (uint32_t d = 0; d < kMaxDims; ++d) c.order[nv][d] = (d < P.n_dims) ? cand[d] : 0u;
             c.n_steps[nv] = make_steps(P, c.order[nv], c.steps[nv]);

@@ -242,13 +242,51 @@ def test_q33_full_size(sj, oracle, engine, full, order):
         assert got == want, (order, lip, bpk, adaptive)
 
 
-def test_adaptive_lip_reorders_bad_plan(sj, engine, full):
-    host, dev = full
-    q = sj.q33_query(FULL, order=(2, 1, 0), bf_bits_per_key=16, adaptive=True)  # D first: 86% pass
-    pq = engine.prepare(q, dev, FULL.fact_rows)
-    pq.build()
-    pq.probe()
-    pq.fetch()
+def _probe_ms(engine, q, cols, rows, reps=5):
+    pq = engine.prepare(q, cols, rows)
+    times = []
+    for _ in range(reps):
+        pq.build()
+        pq.probe()
+        pq.fetch()
+        times.append(pq.stats().probe_ms)
     st = pq.stats()
-    assert st.reorders > 0
+    res = pq.fetch()
     pq.release()
+    return sorted(times)[reps // 2], st, res
+
+
+def test_adaptive_lip_starts_from_the_cheapest_order(sj, engine, full):
+    """With adaptive LIP the starting order comes from each dimension's
+    qualifying fraction: the reference's worst driver order (D first, 86% pass)
+    runs about as fast as the best one."""
+    host, dev = full
+    for bpk in (0, 16):
+        good, _, want = _probe_ms(engine, sj.q33_query(FULL, order=(0, 1, 2), bf_bits_per_key=bpk, adaptive=True),
+                                  dev, FULL.fact_rows)
+        bad, _, got = _probe_ms(engine, sj.q33_query(FULL, order=(2, 1, 0), bf_bits_per_key=bpk, adaptive=True),
+                                dev, FULL.fact_rows)
+        assert got == want
+        assert bad < 1.3 * good + 0.02, (bpk, good, bad)
+
+
+def test_adaptive_lip_reorders_when_the_estimate_misleads(sj, engine, full, torch_cuda):
+    """Supplier FKs skewed onto qualifying suppliers: the supplier filter looks
+    most selective (0.8% of suppliers qualify) but passes most fact rows, so the
+    observed pass rates must re-rank the order during the scan."""
+    torch = torch_cuda
+    host, dev = full
+    n = FULL.fact_rows
+    keys = dev["s_key"][torch.isin(dev["s_city"], torch.tensor([231, 235], device="cuda", dtype=torch.int32))]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    pick = keys[torch.randint(0, keys.numel(), (n,), device="cuda", generator=g)]
+    skew = torch.where(torch.rand(n, device="cuda", generator=g) < 0.95, pick, dev["fk_supp"])
+    cols = dict(dev)
+    cols["fk_supp"] = skew
+    q = sj.q33_query(FULL, order=(0, 1, 2), bf_bits_per_key=16, adaptive=True)
+    _, st, got = _probe_ms(engine, q, cols, n, reps=2)
+    assert st.reorders > 0
+    fixed = sj.q33_query(FULL, order=(1, 0, 2), bf_bits_per_key=16, adaptive=False)
+    _, _, want = _probe_ms(engine, fixed, cols, n, reps=1)
+    assert got == want
