@@ -147,6 +147,7 @@ void cache_put(const char* path, const std::string& sig, const sj_plan& p) {
 
 extern "C" sj_status sj_autotune(sj_engine* eng, sj_plan* plan, const sj_autotune_opts* opts,
                                  sj_autotune_report* report, void* stream) {
+  SjNvtxRange nvtx_range("sj.autotune");
   if (!eng || !plan) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "engine or plan is NULL");
   sj_autotune_opts o{};
   if (opts) o = *opts;

@@ -57,6 +57,7 @@ void schema_release(SchemaState& st) {
 }
 
 sj_status schema_register(sj_engine* eng, const sjb_schema* sc, SchemaState& st) {
+  SjNvtxRange nvtx_range("sjb.schema_register");
   if (!sc) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "schema is NULL");
   if (sc->n_dims < 1 || sc->n_dims > SJ_MAX_DIMS) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "n_dims=%d", sc->n_dims);
   if (!sc->measure || !aligned16(sc->measure) || (sc->measure_sub && !aligned16(sc->measure_sub)))
@@ -377,6 +378,7 @@ static cudaError_t batch_launch(sjb_batch* b, cudaStream_t st) {
 
 extern "C" sj_status sjb_batch_run(sjb_batch* b, const sjb_query* queries, int32_t n, sjb_row* out, int64_t cap,
                                    int64_t* n_out, void* stream) {
+  SjNvtxRange nvtx_range("sjb.batch_run");
   if (!b || !queries || !n_out) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "NULL argument");
   if (n < 1 || n > SJB_MAX_QUERIES) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "n=%d (1..%d)", n, SJB_MAX_QUERIES);
   *n_out = 0;

@@ -68,6 +68,7 @@ extern "C" const char* sj_status_string(sj_status s) {
     case SJ_ERR_TIMEOUT: return "device wait timed out";
     case SJ_ERR_NO_DEVICE: return "no CUDA device";
     case SJ_ERR_REJECTED: return "rejected by admission control";
+    case SJ_ERR_CANCELLED: return "cancelled";
   }
   return "unknown status";
 }
@@ -402,6 +403,7 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
 }
 
 extern "C" sj_status sj_query_build(sj_query* q, void* stream) {
+  SjNvtxRange nvtx_range("sj.query.build");
   if (!q) return fail(SJ_ERR_INVALID_ARGUMENT, "NULL query");
   cudaStream_t st = (cudaStream_t)stream;
   SJ_CUDA(cudaSetDevice(q->eng->device));
@@ -427,6 +429,7 @@ extern "C" sj_status sj_query_build(sj_query* q, void* stream) {
 }
 
 extern "C" sj_status sj_query_probe(sj_query* q, void* stream) {
+  SjNvtxRange nvtx_range("sj.query.probe");
   if (!q) return fail(SJ_ERR_INVALID_ARGUMENT, "NULL query");
   if (!q->built) return fail(SJ_ERR_INVALID_ARGUMENT, "probe before build");
   cudaStream_t st = (cudaStream_t)stream;
@@ -448,6 +451,7 @@ static bool row_less(const sj_group_row& a, const sj_group_row& b) {
 }
 
 extern "C" sj_status sj_query_fetch(sj_query* q, sj_group_row* out, int64_t cap, int64_t* n_out, void* stream) {
+  SjNvtxRange nvtx_range("sj.query.fetch");
   if (!q || !n_out) return fail(SJ_ERR_INVALID_ARGUMENT, "NULL query/n_out");
   if (!q->probed) return fail(SJ_ERR_INVALID_ARGUMENT, "fetch before probe");
   cudaStream_t st = (cudaStream_t)stream;
@@ -578,6 +582,7 @@ static sj_status run_query_whole(sj_engine* eng, const sj_plan& p, sj_group_row*
 // host memory and are read in place at survivor rows only.
 static sj_status run_query_streamed(sj_engine* eng, sj_plan p, const int32_t* host_first, sj_group_row* out,
                                     int64_t cap, int64_t* n_out, cudaStream_t st, cudaEvent_t t1) {
+  SjNvtxRange nvtx_range("sj.run_plain.streamed");
   const int first = p.order[0];
   const int64_t b = p.row_begin, e = p.row_end;
   const int64_t base = b & ~3ll;
@@ -635,6 +640,7 @@ static sj_status run_query_streamed(sj_engine* eng, sj_plan p, const int32_t* ho
 
 extern "C" sj_status sj_run_plain(sj_engine* eng, const sj_plan* plan, int host_columns, sj_group_row* out,
                                   int64_t cap, int64_t* n_out, float* ms, void* stream) {
+  SjNvtxRange nvtx_range("sj.run_plain");
   if (!eng || !plan || !n_out) return fail(SJ_ERR_INVALID_ARGUMENT, "NULL engine/plan/n_out");
   cudaStream_t st = (cudaStream_t)stream;
   SJ_CUDA(cudaSetDevice(eng->device));

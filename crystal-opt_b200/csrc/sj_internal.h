@@ -6,6 +6,16 @@
 #include "../../include/starjoin.h"
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
+
+// Named range on the host timeline for each stage (NVTX v3, header-only: free
+// unless a profiler is attached).
+struct SjNvtxRange {
+  explicit SjNvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~SjNvtxRange() { nvtxRangePop(); }
+  SjNvtxRange(const SjNvtxRange&) = delete;
+  SjNvtxRange& operator=(const SjNvtxRange&) = delete;
+};
 
 // Engine handle of the C ABI (include/starjoin.h): one device, one memory pool.
 struct sj_engine {

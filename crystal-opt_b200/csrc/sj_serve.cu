@@ -45,6 +45,7 @@ struct Ticket {
   double submit_s = 0, admit_s = 0, finish_s = 0;
   int status = SJ_OK;
   bool done = false;
+  bool cancel = false;  // asked to leave the scan (sjs_cancel)
   std::vector<sjb_row> rows;
 };
 
@@ -62,6 +63,7 @@ struct Slot {
   float sel[SJ_MAX_DIMS] = {1.f, 1.f, 1.f, 1.f};
   const uint32_t* bm[SJ_MAX_DIMS] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<Interval> remaining;  // fact rows still to scan (at most two pieces)
+  bool cancelled = false;           // leaves at the next step boundary; groups discarded
 };
 
 }  // namespace
@@ -113,6 +115,8 @@ struct sjs_server {
   std::unordered_map<uint64_t, Ticket> tickets;
   uint64_t next_ticket = 1;
   bool stop = false;
+  int waiters = 0;             // threads inside sjs_wait
+  uint64_t admissions = 0;     // admission attempts (fault injection counts these)
   Slot slots[kBq];
   bool masks_dirty = true;
   sjs_stats stats{};
@@ -193,6 +197,7 @@ void release_slot(sjs_server* s, int q) {
 
 // Admit pending tickets into free slots while memory allows.  Returns false on a CUDA error.
 bool admit(sjs_server* s) {
+  SjNvtxRange nvtx_range("sjs.admit");
   std::vector<uint64_t> cand;
   bool idle = true;
   for (const Slot& sl : s->slots) idle &= !sl.used;
@@ -220,6 +225,15 @@ bool admit(sjs_server* s) {
     {
       std::lock_guard<std::mutex> g(s->mu);
       t = &s->tickets[id];
+    }
+    if (s->cfg.fault_admit_every > 0 && ++s->admissions % (uint64_t)s->cfg.fault_admit_every == 0) {
+      // injected fault: this admission fails as a device allocation would
+      {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->pending.erase(std::find(s->pending.begin(), s->pending.end(), id));
+      }
+      finish_ticket(s, id, SJ_ERR_OUT_OF_MEMORY, {});
+      continue;
     }
     Adm a{id, {-1, -1, -1, -1}, 0};
     bool ok = true;
@@ -425,6 +439,7 @@ void fill_step(sjs_server* s, SjbStep& st, bool all, int64_t seg_b, int64_t seg_
 // compaction and copies go into the stream right behind the probe; the host
 // collects them (complete_step) while the next step already runs.
 bool launch_step(sjs_server* s, bool* launched) {
+  SjNvtxRange nvtx_range("sjs.launch_step");
   *launched = false;
   const int b = s->next_buf;
   const int64_t n = s->S.rt.fact_rows;
@@ -491,6 +506,7 @@ bool launch_step(sjs_server* s, bool* launched) {
 
 // Wait for the step in buffer set `b` and hand out the groups it read back.
 bool complete_step(sjs_server* s, int b) {
+  SjNvtxRange nvtx_range("sjs.complete_step");
   auto& r = s->rec[b];
   if (!r.valid) return true;
   if (cudaEventSynchronize(s->ev_done[b]) != cudaSuccess) return false;
@@ -504,9 +520,11 @@ bool complete_step(sjs_server* s, int b) {
       if (!((r.fin >> q) & 1ull)) continue;
       for (sjb_row& x : per[q]) x.query = 0;
       const uint64_t id = s->slots[q].ticket;
+      const bool cancelled = s->slots[q].cancelled;
       release_slot(s, q);
       s->fin_queued &= ~(1ull << q);
-      finish_ticket(s, id, SJ_OK, std::move(per[q]));
+      if (cancelled) per[q].clear();
+      finish_ticket(s, id, cancelled ? SJ_ERR_CANCELLED : SJ_OK, std::move(per[q]));
     }
   }
   if (r.probed) {
@@ -521,6 +539,7 @@ bool complete_step(sjs_server* s, int b) {
 }
 
 void plain_one(sjs_server* s, uint64_t id) {
+  SjNvtxRange nvtx_range("sjs.plain_query");
   Ticket* t;
   {
     std::lock_guard<std::mutex> g(s->mu);
@@ -616,6 +635,18 @@ void loop(sjs_server* s) {
       const double t1 = now_s();
       bool active = false;
       for (const Slot& sl : s->slots) active |= sl.used;
+      {  // running queries asked to stop leave the scan: nothing left to read
+        std::lock_guard<std::mutex> g(s->mu);
+        for (Slot& sl : s->slots) {
+          if (!sl.used || sl.cancelled) continue;
+          auto it = s->tickets.find(sl.ticket);
+          if (it != s->tickets.end() && it->second.cancel) {
+            sl.cancelled = true;
+            sl.remaining.clear();
+            s->masks_dirty = true;
+          }
+        }
+      }
       bool launched = false;
       if (ok && active) ok = launch_step(s, &launched);
       if (ok && launched) ok = complete_step(s, s->next_buf);  // the older of the two buffer sets
@@ -826,15 +857,39 @@ extern "C" sj_status sjs_wait(sjs_server* s, uint64_t ticket, double timeout_s, 
   auto it = s->tickets.find(ticket);
   if (it == s->tickets.end()) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "unknown ticket %llu", (unsigned long long)ticket);
   auto ready = [&] { return it->second.done; };
-  if (timeout_s > 0) {
-    if (!s->cv_done.wait_for(g, std::chrono::duration<double>(timeout_s), ready)) {
-      take_result(s, it->second, ticket, info, nullptr, 0);
-      return fail_fmt(SJ_ERR_TIMEOUT, "ticket %llu not finished after %.3f s", (unsigned long long)ticket, timeout_s);
-    }
+  ++s->waiters;
+  sj_status rc;
+  if (timeout_s > 0 && !s->cv_done.wait_for(g, std::chrono::duration<double>(timeout_s), ready)) {
+    take_result(s, it->second, ticket, info, nullptr, 0);
+    rc = fail_fmt(SJ_ERR_TIMEOUT, "ticket %llu not finished after %.3f s", (unsigned long long)ticket, timeout_s);
   } else {
-    s->cv_done.wait(g, ready);
+    if (timeout_s <= 0) s->cv_done.wait(g, ready);
+    rc = take_result(s, it->second, ticket, info, out, cap);
   }
-  return take_result(s, it->second, ticket, info, out, cap);
+  --s->waiters;
+  s->cv_done.notify_all();
+  return rc;
+}
+
+extern "C" sj_status sjs_cancel(sjs_server* s, uint64_t ticket) {
+  if (!s) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "NULL server");
+  std::lock_guard<std::mutex> g(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "unknown ticket %llu", (unsigned long long)ticket);
+  Ticket& t = it->second;
+  if (t.done) return SJ_OK;
+  auto p = std::find(s->pending.begin(), s->pending.end(), ticket);
+  if (p != s->pending.end()) {  // not admitted yet: drop it here
+    s->pending.erase(p);
+    t.done = true;
+    t.status = SJ_ERR_CANCELLED;
+    t.finish_s = now_s();
+    ++s->stats.finished;
+    s->cv_done.notify_all();
+    return SJ_OK;
+  }
+  t.cancel = true;  // running: the loop takes it out of the scan
+  return SJ_OK;
 }
 
 extern "C" sj_status sjs_get_stats(sjs_server* s, sjs_stats* out) {
@@ -852,6 +907,18 @@ extern "C" void sjs_server_destroy(sjs_server* s) {
   }
   s->cv_work.notify_all();
   if (s->th.joinable()) s->th.join();
+  {
+    std::unique_lock<std::mutex> g(s->mu);
+    for (auto& kv : s->tickets)
+      if (!kv.second.done) {
+        kv.second.done = true;
+        kv.second.status = SJ_ERR_CANCELLED;
+        kv.second.finish_s = now_s();
+      }
+    s->pending.clear();
+    s->cv_done.notify_all();
+    s->cv_done.wait(g, [&] { return s->waiters == 0; });
+  }
   for (int q = 0; q < kBq; ++q)
     if (s->slots[q].used) release_slot(s, q);
   server_free(s);

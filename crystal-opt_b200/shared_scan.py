@@ -61,7 +61,8 @@ class SjbStats(C.Structure):
 
 class SjsConfig(C.Structure):
     _fields_ = [("limits", SjbLimits), ("step_rows", C.c_int64), ("max_active", C.c_int32),
-                ("plain", C.c_int32), ("hbm_reserve_bytes", C.c_int64)]
+                ("plain", C.c_int32), ("hbm_reserve_bytes", C.c_int64), ("fault_admit_every", C.c_int32),
+                ("pad_", C.c_int32)]
 
 
 class SjsTicketInfo(C.Structure):
@@ -78,7 +79,7 @@ class SjsStats(C.Structure):
 
 
 SYMBOLS = ["sjb_batch_create", "sjb_batch_destroy", "sjb_batch_run", "sjb_batch_get_stats",
-           "sjs_server_create", "sjs_submit", "sjs_poll", "sjs_wait", "sjs_get_stats", "sjs_now",
+           "sjs_server_create", "sjs_submit", "sjs_poll", "sjs_wait", "sjs_cancel", "sjs_get_stats", "sjs_now",
            "sjs_server_destroy"]
 
 
@@ -98,6 +99,7 @@ def load() -> C.CDLL:
         "sjs_poll": (C.c_int, [P, C.c_uint64, C.POINTER(SjsTicketInfo), C.POINTER(SjbRow), C.c_int64]),
         "sjs_wait": (C.c_int, [P, C.c_uint64, C.c_double, C.POINTER(SjsTicketInfo), C.POINTER(SjbRow),
                                C.c_int64]),
+        "sjs_cancel": (C.c_int, [P, C.c_uint64]),
         "sjs_get_stats": (C.c_int, [P, C.POINTER(SjsStats)]),
         "sjs_now": (C.c_double, []),
         "sjs_server_destroy": (None, [P]),
@@ -337,7 +339,7 @@ class Server:
 
     def __init__(self, eng: sj.Engine, schema: sj.StarSchema, cols: Dict[str, Any], plain=False, step_rows=0,
                  max_active=0, cache_filters=True, group_entries=0, filter_cache_bytes=0, threads=0,
-                 hbm_reserve_bytes=0):
+                 hbm_reserve_bytes=0, fault_admit_every=0):
         self.lib = load()
         self.eng, self.schema = eng, schema
         self._schema, self._keep = make_schema(schema, cols)
@@ -347,6 +349,7 @@ class Server:
         cfg.max_active = max_active
         cfg.plain = 1 if plain else 0
         cfg.hbm_reserve_bytes = hbm_reserve_bytes
+        cfg.fault_admit_every = fault_admit_every
         h = C.c_void_p()
         sj.check(self.lib.sjs_server_create(eng.h, C.byref(self._schema), C.byref(cfg), C.byref(h)))
         self.h = h
@@ -368,6 +371,9 @@ class Server:
         sj.check(self.lib.sjs_wait(self.h, ticket, timeout_s, C.byref(info), rows, cap))
         q = self.queries.pop(ticket)
         return rows_by_query_one(rows, info.n_rows, q), info
+
+    def cancel(self, ticket: int) -> None:
+        sj.check(self.lib.sjs_cancel(self.h, ticket))
 
     def stats(self) -> SjsStats:
         s = SjsStats()

@@ -31,6 +31,7 @@ SJ_ERR_CAPACITY = 5
 SJ_ERR_TIMEOUT = 6
 SJ_ERR_NO_DEVICE = 7
 SJ_ERR_REJECTED = 8
+SJ_ERR_CANCELLED = 9
 
 PRED_ALL, PRED_IN, PRED_RANGE = 0, 1, 2
 

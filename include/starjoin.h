@@ -58,7 +58,8 @@ typedef enum sj_status {
   SJ_ERR_CAPACITY = 5,   /* caller's result buffer is too small; *n_out holds the need */
   SJ_ERR_TIMEOUT = 6,    /* a bounded device-side wait expired; context stays usable */
   SJ_ERR_NO_DEVICE = 7,  /* no CUDA device / extension built without one */
-  SJ_ERR_REJECTED = 8    /* admission control refused the request (serving form) */
+  SJ_ERR_REJECTED = 8,   /* admission control refused the request (serving form) */
+  SJ_ERR_CANCELLED = 9   /* the request was cancelled, or its server shut down (serving form) */
 } sj_status;
 
 /* Dimension predicate kinds (the reference's BlockPred* chains in the build

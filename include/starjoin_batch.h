@@ -132,6 +132,9 @@ typedef struct sjs_config {
   int32_t max_active;                /* queries sharing the scan (1..SJB_MAX_QUERIES, 0 = 64) */
   int32_t plain;                     /* 1: one query at a time through the plain engine (the baseline loop) */
   int64_t hbm_reserve_bytes;         /* device memory left free for others (0 = 2 GiB) */
+  int32_t fault_admit_every;         /* fault injection (tests): every k-th admission fails as if its
+                                        device allocation had failed (SJ_ERR_OUT_OF_MEMORY); 0 = off */
+  int32_t pad_;
 } sjs_config;
 
 typedef struct sjs_ticket_info {
@@ -162,8 +165,14 @@ sj_status sjs_poll(sjs_server* s, uint64_t ticket, sjs_ticket_info* info, sjb_ro
 /* Block until the ticket is done (timeout_s <= 0: no limit), then as sjs_poll. */
 sj_status sjs_wait(sjs_server* s, uint64_t ticket, double timeout_s, sjs_ticket_info* info, sjb_row* out,
                    int64_t cap);
+/* Cancel a ticket: a queued query is dropped, a running one leaves the scan at
+ * the next step boundary; either way the ticket completes with SJ_ERR_CANCELLED.
+ * Cancelling a finished ticket changes nothing. */
+sj_status sjs_cancel(sjs_server* s, uint64_t ticket);
 sj_status sjs_get_stats(sjs_server* s, sjs_stats* out);
 double sjs_now(void);                /* the clock of sjs_ticket_info, seconds */
+/* Stops the loop; open tickets complete with SJ_ERR_CANCELLED and threads
+ * blocked in sjs_wait return before the server is freed. */
 void sjs_server_destroy(sjs_server* s);
 
 #ifdef __cplusplus

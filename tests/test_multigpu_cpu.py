@@ -4,6 +4,7 @@ same all-gather the multi-GPU benchmark uses; the merge must equal a single run
 over the whole table, bit for bit."""
 import os
 import socket
+import time
 
 import pytest
 import torch.distributed as dist
@@ -70,3 +71,39 @@ def test_two_gloo_ranks_merge_to_the_single_run(sj, oracle, world):
         want = oracle.run(sj.q33_query(sc, cities=cities), cols)
         for r in range(world):
             assert out[r][i] == want
+
+
+def _dying_rank(rank, world, port, out):
+    import datetime
+    import sys
+    for sub in ("crystal-opt_b200",):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    import multigpu
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    if rank == 1:
+        os._exit(3)  # the worker dies between steps, before the exchange
+    t0 = time.time()
+    try:
+        multigpu.merge_groups([(1, 2, 3, 4, 5)], 3, dist)
+        out[rank] = ("merged", time.time() - t0)
+    except Exception as e:  # noqa: BLE001
+        out[rank] = ("error", time.time() - t0, type(e).__name__)
+
+
+def test_surviving_rank_learns_of_a_dead_worker():
+    """A rank that exits before the group merge: the surviving rank's collective
+    ends with an error within the process-group timeout instead of hanging."""
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    port = _free_port()
+    ctx = mp.start_processes(_dying_rank, args=(2, port, out), nprocs=2, join=False, start_method="spawn")
+    deadline = time.time() + 60
+    for p in ctx.processes:
+        p.join(timeout=max(1.0, deadline - time.time()))
+    alive = [p for p in ctx.processes if p.is_alive()]
+    for p in alive:
+        p.kill()
+    assert not alive
+    assert ctx.processes[1].exitcode == 3
+    assert out[0][0] == "error" and out[0][1] < 30

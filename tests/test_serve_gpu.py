@@ -120,3 +120,76 @@ def test_concurrent_submitters(oracle, engine, star):
     assert len(results) == 24
     for q, rows in results.values():
         assert rows == oracle.run(ss.to_plain(sc, q), host)
+
+
+def test_cancel_queued_and_running(sj, oracle, engine, star):
+    """Cancelled tickets complete with SJ_ERR_CANCELLED (or with their full,
+    correct result if they finished first); every other query is unaffected."""
+    sc, host, dev = star
+    rng = random.Random(14)
+    qs = [ss.random_query(rng, sc, len_range=(1_000_000, None)) for _ in range(40)]
+    srv = ss.Server(engine, sc, dev, step_rows=1 << 18, max_active=8)
+    try:
+        tickets = [srv.submit(q) for q in qs]
+        for t in tickets[::3]:
+            srv.cancel(t)
+        cancelled = 0
+        for i, (q, t) in enumerate(zip(qs, tickets)):
+            try:
+                rows, _ = srv.wait(t, timeout_s=120.0)
+            except sj.StarJoinError as e:
+                assert i % 3 == 0 and e.status == sj.SJ_ERR_CANCELLED, (i, e)
+                cancelled += 1
+                continue
+            assert rows == oracle.run(ss.to_plain(sc, q), host), i
+        assert cancelled >= 7  # with 8 slots most of the 14 cancelled tickets were still queued
+    finally:
+        srv.close()
+
+
+def test_injected_allocation_failures(sj, oracle, engine, star):
+    """Fault injection on the host: every 3rd admission fails as its device
+    allocation would; those tickets report SJ_ERR_OUT_OF_MEMORY, the server keeps
+    serving, and every other result stays exact."""
+    sc, host, dev = star
+    rng = random.Random(15)
+    qs = [ss.random_query(rng, sc, len_range=(100_000, None)) for _ in range(24)]
+    srv = ss.Server(engine, sc, dev, fault_admit_every=3, step_rows=1 << 19)
+    try:
+        tickets = [srv.submit(q) for q in qs]
+        failed = 0
+        for q, t in zip(qs, tickets):
+            try:
+                rows, _ = srv.wait(t, timeout_s=120.0)
+            except sj.StarJoinError as e:
+                assert e.status == sj.SJ_ERR_OUT_OF_MEMORY
+                failed += 1
+                continue
+            assert rows == oracle.run(ss.to_plain(sc, q), host)
+        assert failed == 8
+    finally:
+        srv.close()
+
+
+def test_destroy_releases_blocked_waiters(sj, engine, star):
+    sc, _, dev = star
+    rng = random.Random(16)
+    qs = [ss.random_query(rng, sc, len_range=(2_000_000, None)) for _ in range(64)]
+    srv = ss.Server(engine, sc, dev, step_rows=1 << 17, max_active=2)
+    tickets = [srv.submit(q) for q in qs]
+    outcome = {}
+
+    def waiter():
+        try:
+            srv.wait(tickets[-1])  # no timeout: only the shutdown can end this wait early
+            outcome["status"] = 0
+        except sj.StarJoinError as e:
+            outcome["status"] = e.status
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    time.sleep(0.05)
+    srv.close()
+    th.join(timeout=30)
+    assert not th.is_alive()
+    assert outcome["status"] in (0, sj.SJ_ERR_CANCELLED)
