@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <climits>
 #include <map>
 #include <string>
 #include <unordered_map>
@@ -69,6 +70,70 @@ class RangeAlloc {
   uint64_t align_ = 1, cap_ = 0, used_ = 0;
   std::map<uint64_t, uint64_t> free_;
 };
+
+// Coverage bookkeeping of a query on the circular scan: the fact rows it still
+// needs, as at most two disjoint intervals (the part of [b, e) after its attach
+// point, then the part before it, reached after the scan wraps).
+struct Interval {
+  int64_t b, e;
+};
+
+// Rows [b, e) intersected with the rows still to scan, one piece (a scan step
+// never wraps, so at most one piece is non-empty).
+inline Interval take(const std::vector<Interval>& remaining, int64_t b, int64_t e) {
+  for (const Interval& iv : remaining) {
+    const int64_t lo = std::max(iv.b, b), hi = std::min(iv.e, e);
+    if (lo < hi) return {lo, hi};
+  }
+  return {0, 0};
+}
+
+// Remove the scanned rows c from the remaining intervals.
+inline void cover(std::vector<Interval>& remaining, Interval c) {
+  std::vector<Interval> out;
+  for (const Interval& iv : remaining) {
+    if (c.e <= iv.b || c.b >= iv.e) {
+      out.push_back(iv);
+      continue;
+    }
+    if (iv.b < c.b) out.push_back({iv.b, c.b});
+    if (c.e < iv.e) out.push_back({c.e, iv.e});
+  }
+  remaining.swap(out);
+}
+
+// The intervals a query attaching at scan position p needs for [b, e): rows
+// [p, e) first, then [b, p) after the wrap.
+inline std::vector<Interval> attach(int64_t b, int64_t e, int64_t p) {
+  if (e <= b) return {};
+  if (p > b && p < e) return {{p, e}, {b, p}};
+  return {{b, e}};
+}
+
+// First row at or after `pos` (cyclically over [0, n)) in the intervals, and
+// its cyclic distance from pos; -1 when nothing is left.
+inline int64_t first_needed(const std::vector<Interval>& remaining, int64_t pos, int64_t n, int64_t* dist) {
+  int64_t best = -1, best_dist = INT64_MAX;
+  for (const Interval& iv : remaining) {
+    int64_t cand, d;
+    if (pos >= iv.b && pos < iv.e) {
+      cand = pos;
+      d = 0;
+    } else if (iv.b >= pos) {
+      cand = iv.b;
+      d = iv.b - pos;
+    } else {
+      cand = iv.b;
+      d = iv.b + n - pos;
+    }
+    if (d < best_dist) {
+      best_dist = d;
+      best = cand;
+    }
+  }
+  *dist = best_dist;
+  return best;
+}
 
 // Filter bitmaps (one bit per PHT slot) and their statistics, resident on the
 // device and shared by every query with the same dimension predicate.

@@ -116,6 +116,12 @@ extern "C" sj_status sj_engine_create(int device, sj_engine** out) {
   }
   uint64_t thr = ~0ull;  // keep freed blocks for reuse by later queries
   cudaMemPoolSetAttribute(eng->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  e = cudaStreamCreateWithFlags(&eng->copy_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    cudaMemPoolDestroy(eng->pool);
+    delete eng;
+    return fail(SJ_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+  }
   *out = eng;
   return SJ_OK;
 }
@@ -596,7 +602,6 @@ static sj_status run_query_streamed(sj_engine* eng, sj_plan p, const int32_t* ho
   std::vector<cudaEvent_t> evs;
   if (s == SJ_OK) s = sj_query_build(q, st);
   if (s == SJ_OK) {
-    if (!eng->copy_stream) cudaStreamCreateWithFlags(&eng->copy_stream, cudaStreamNonBlocking);
     cs = eng->copy_stream;
     cudaEvent_t ready;
     cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);

@@ -23,7 +23,7 @@ struct sj_engine {
   int sm_count = 148;
   size_t smem_optin = 232448;
   cudaMemPool_t pool = nullptr;
-  cudaStream_t copy_stream = nullptr;  // host->device staging of streamed columns (created on first use)
+  cudaStream_t copy_stream = nullptr;  // host->device staging of streamed columns
 };
 
 namespace sj {

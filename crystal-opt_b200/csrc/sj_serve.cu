@@ -49,10 +49,6 @@ struct Ticket {
   std::vector<sjb_row> rows;
 };
 
-struct Interval {
-  int64_t b, e;
-};
-
 struct Slot {
   bool used = false;
   uint64_t ticket = 0;
@@ -138,50 +134,16 @@ void finish_ticket(sjs_server* s, uint64_t id, int status, std::vector<sjb_row>&
   s->cv_done.notify_all();
 }
 
-// Rows [b, e) intersected with the rows still to scan, one piece (the scan
-// never wraps inside a step, so at most one piece is non-empty).
-Interval take(const Slot& sl, int64_t b, int64_t e) {
-  for (const Interval& iv : sl.remaining) {
-    const int64_t lo = std::max(iv.b, b), hi = std::min(iv.e, e);
-    if (lo < hi) return {lo, hi};
-  }
-  return {0, 0};
-}
-
-void cover(Slot& sl, Interval c) {
-  std::vector<Interval> out;
-  for (const Interval& iv : sl.remaining) {
-    if (c.e <= iv.b || c.b >= iv.e) {
-      out.push_back(iv);
-      continue;
-    }
-    if (iv.b < c.b) out.push_back({iv.b, c.b});
-    if (c.e < iv.e) out.push_back({c.e, iv.e});
-  }
-  sl.remaining.swap(out);
-}
-
 // Next row at or after `pos` (cyclically over [0, n)) that an admitted query still needs.
 int64_t next_needed(sjs_server* s, int64_t pos, int64_t n) {
   int64_t best = -1, best_dist = INT64_MAX;
   for (const Slot& sl : s->slots) {
     if (!sl.used) continue;
-    for (const Interval& iv : sl.remaining) {
-      int64_t cand, dist;
-      if (pos >= iv.b && pos < iv.e) {
-        cand = pos;
-        dist = 0;
-      } else if (iv.b >= pos) {
-        cand = iv.b;
-        dist = iv.b - pos;
-      } else {
-        cand = iv.b;
-        dist = iv.b + n - pos;
-      }
-      if (dist < best_dist) {
-        best_dist = dist;
-        best = cand;
-      }
+    int64_t dist = 0;
+    const int64_t cand = first_needed(sl.remaining, pos, n, &dist);
+    if (cand >= 0 && dist < best_dist) {
+      best_dist = dist;
+      best = cand;
     }
   }
   return best;
@@ -193,6 +155,32 @@ void release_slot(sjs_server* s, int q) {
   if (sl.group_span) s->groups.release(sl.group_off, sl.group_span);
   sl = Slot();
   s->masks_dirty = true;
+}
+
+// A pending ticket's query, copied under s->mu (the ticket itself may be
+// cancelled and released while the copy is in use).
+struct QueryCopy {
+  sjb_query q{};
+  std::vector<int32_t> codes[SJ_MAX_DIMS];
+};
+
+bool pending_query(sjs_server* s, uint64_t id, QueryCopy& out) {
+  auto it = s->tickets.find(id);
+  if (it == s->tickets.end() || it->second.done) return false;
+  out.q = it->second.q;
+  for (int k = 0; k < SJ_MAX_DIMS; ++k) {
+    out.codes[k] = it->second.codes[k];
+    if (k < out.q.n_preds && out.q.preds[k].in_count > 0) out.q.preds[k].in_codes = out.codes[k].data();
+  }
+  return true;
+}
+
+// Remove id from the queue (under s->mu); false if it left meanwhile (cancelled).
+bool take_pending(sjs_server* s, uint64_t id) {
+  auto p = std::find(s->pending.begin(), s->pending.end(), id);
+  if (p == s->pending.end()) return false;
+  s->pending.erase(p);
+  return true;
 }
 
 // Admit pending tickets into free slots while memory allows.  Returns false on a CUDA error.
@@ -213,6 +201,7 @@ bool admit(sjs_server* s) {
     uint64_t id;
     int entry[SJ_MAX_DIMS];
     int n;
+    QueryCopy qc;
   };
   std::vector<Adm> adm;
   SjbBatchDesc& D = *s->desc_h;
@@ -221,24 +210,25 @@ bool admit(sjs_server* s) {
   uint64_t hits = 0;
   std::vector<int> new_ids;
   for (uint64_t id : cand) {
-    Ticket* t;
+    Adm a{id, {-1, -1, -1, -1}, 0, {}};
     {
       std::lock_guard<std::mutex> g(s->mu);
-      t = &s->tickets[id];
+      if (!pending_query(s, id, a.qc)) continue;  // cancelled since the queue was read
     }
     if (s->cfg.fault_admit_every > 0 && ++s->admissions % (uint64_t)s->cfg.fault_admit_every == 0) {
       // injected fault: this admission fails as a device allocation would
+      bool was;
       {
         std::lock_guard<std::mutex> g(s->mu);
-        s->pending.erase(std::find(s->pending.begin(), s->pending.end(), id));
+        was = take_pending(s, id);
       }
-      finish_ticket(s, id, SJ_ERR_OUT_OF_MEMORY, {});
+      if (was) finish_ticket(s, id, SJ_ERR_OUT_OF_MEMORY, {});
       continue;
     }
-    Adm a{id, {-1, -1, -1, -1}, 0};
+    const sjb_query& tq = a.qc.q;
     bool ok = true;
-    for (int k = 0; k < t->q.n_preds && ok; ++k) {
-      const sjb_pred& p = t->q.preds[k];
+    for (int k = 0; k < tq.n_preds && ok; ++k) {
+      const sjb_pred& p = tq.preds[k];
       bool is_new = false;
       const int eid = s->cache.acquire(p, s->S.words[p.dim], s->cfg.limits.cache_filters != 0, &is_new);
       if (eid < 0 || (is_new && (D.n_jobs >= (uint32_t)kBMaxJobs ||
@@ -274,16 +264,17 @@ bool admit(sjs_server* s) {
     if (!ok) {
       for (int k = 0; k < a.n; ++k) s->cache.release(a.entry[k]);
       if (idle && adm.empty()) {  // cannot fit even alone: refuse it
+        bool was;
         {
           std::lock_guard<std::mutex> g(s->mu);
-          s->pending.erase(std::find(s->pending.begin(), s->pending.end(), id));
-          ++s->stats.rejected;
+          was = take_pending(s, id);
+          if (was) ++s->stats.rejected;
         }
-        finish_ticket(s, id, SJ_ERR_REJECTED, {});
+        if (was) finish_ticket(s, id, SJ_ERR_REJECTED, {});
       }
       break;  // memory is full: keep FIFO order, retry after queries leave
     }
-    adm.push_back(a);
+    adm.push_back(std::move(a));
   }
   // build the new filters and read back every admitted predicate's statistics
   if (D.n_jobs) {
@@ -314,19 +305,15 @@ bool admit(sjs_server* s) {
   // group layout and accumulator ranges
   const double t_adm = now_s();
   for (const Adm& a : adm) {
-    Ticket* t;
-    {
-      std::lock_guard<std::mutex> g(s->mu);
-      t = &s->tickets[a.id];
-    }
+    const sjb_query& tq = a.qc.q;
     SjbBatchQuery bq{};
-    bq.b = t->q.row_begin;
-    bq.e = t->q.row_end;
-    bq.n_preds = (uint32_t)t->q.n_preds;
+    bq.b = tq.row_begin;
+    bq.e = tq.row_end;
+    bq.n_preds = (uint32_t)tq.n_preds;
     const SjbEntryStats* stp[SJ_MAX_DIMS];
     for (int k = 0; k < a.n; ++k) {
-      bq.dim[k] = (uint32_t)t->q.preds[k].dim;
-      bq.group_attr[k] = t->q.preds[k].group_attr;
+      bq.dim[k] = (uint32_t)tq.preds[k].dim;
+      bq.group_attr[k] = tq.preds[k].group_attr;
       stp[k] = &s->cache.at(a.entry[k]).host;
     }
     SjbSlot lay{};
@@ -343,21 +330,30 @@ bool admit(sjs_server* s) {
         bool any = false;
         for (const Slot& sl : s->slots) any |= sl.used;
         if (!any) {  // cannot fit even alone: refuse it
+          bool was;
           {
             std::lock_guard<std::mutex> g(s->mu);
-            s->pending.erase(std::find(s->pending.begin(), s->pending.end(), a.id));
-            ++s->stats.rejected;
+            was = take_pending(s, a.id);
+            if (was) ++s->stats.rejected;
           }
-          finish_ticket(s, a.id, SJ_ERR_REJECTED, {});
+          if (was) finish_ticket(s, a.id, SJ_ERR_REJECTED, {});
         }
         break;
       }
     }
+    bool still;
     {
       std::lock_guard<std::mutex> g(s->mu);
-      s->pending.erase(std::find(s->pending.begin(), s->pending.end(), a.id));
-      t->admit_s = t_adm;
-      ++s->stats.admitted;
+      still = take_pending(s, a.id);
+      if (still) {
+        s->tickets[a.id].admit_s = t_adm;
+        ++s->stats.admitted;
+      }
+    }
+    if (!still) {  // cancelled while its filters were built
+      if (span && !err) s->groups.release(off, span);
+      for (int k = 0; k < a.n; ++k) s->cache.release(a.entry[k]);
+      continue;
     }
     if (err || span == 0 || bq.e <= bq.b) {  // no row can match (or key space too large)
       for (int k = 0; k < a.n; ++k) s->cache.release(a.entry[k]);
@@ -381,11 +377,7 @@ bool admit(sjs_server* s) {
     sl.lay.group_base = off;
     // the next step starts at next_pos: rows [next_pos, e) come first, then [b, next_pos) after the wrap
     const int64_t b = bq.b, e = bq.e, p = s->next_pos;
-    if (p > b && p < e) {
-      sl.remaining = {{p, e}, {b, p}};
-    } else {
-      sl.remaining = {{b, e}};
-    }
+    sl.remaining = attach(b, e, p);
     if (cudaMemsetAsync(s->acc + off, 0, sizeof(SjbAcc) * span, s->stb) != cudaSuccess) return false;
     s->masks_dirty = true;
   }
@@ -421,7 +413,7 @@ void fill_step(sjs_server* s, SjbStep& st, bool all, int64_t seg_b, int64_t seg_
       else for (int d = 0; d < SJ_MAX_DIMS; ++d) st.bm[q][d] = nullptr;
       continue;
     }
-    const Interval iv = take(sl, seg_b, seg_e);
+    const Interval iv = take(sl.remaining, seg_b, seg_e);
     if (iv.e > iv.b) {
       st.slot[q].b = iv.b;
       st.slot[q].e = iv.e;
@@ -467,7 +459,7 @@ bool launch_step(sjs_server* s, bool* launched) {
       return false;
     if (cudaEventRecord(s->ev_probe[b][1], s->st) != cudaSuccess) return false;
     for (int q = 0; q < kBq; ++q)
-      if ((st.active >> q) & 1ull) cover(s->slots[q], {st.slot[q].b, st.slot[q].e});
+      if ((st.active >> q) & 1ull) cover(s->slots[q].remaining, {st.slot[q].b, st.slot[q].e});
     s->next_pos = seg_e >= n ? 0 : seg_e;
     probed = true;
   }
@@ -540,15 +532,16 @@ bool complete_step(sjs_server* s, int b) {
 
 void plain_one(sjs_server* s, uint64_t id) {
   SjNvtxRange nvtx_range("sjs.plain_query");
-  Ticket* t;
+  QueryCopy qc;
   {
     std::lock_guard<std::mutex> g(s->mu);
+    if (s->pending.empty() || s->pending.front() != id) return;  // cancelled meanwhile
     s->pending.pop_front();
-    t = &s->tickets[id];
-    t->admit_s = now_s();
+    if (!pending_query(s, id, qc)) return;
+    s->tickets[id].admit_s = now_s();
     ++s->stats.admitted;
   }
-  const sjb_query& q = t->q;
+  const sjb_query& q = qc.q;
   sj_plan plan;
   memset(&plan, 0, sizeof(plan));
   plan.n_dims = q.n_preds;
@@ -856,15 +849,16 @@ extern "C" sj_status sjs_wait(sjs_server* s, uint64_t ticket, double timeout_s, 
   std::unique_lock<std::mutex> g(s->mu);
   auto it = s->tickets.find(ticket);
   if (it == s->tickets.end()) return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "unknown ticket %llu", (unsigned long long)ticket);
-  auto ready = [&] { return it->second.done; };
+  Ticket& t = it->second;  // references survive a rehash by concurrent submits; iterators do not
+  auto ready = [&] { return t.done; };
   ++s->waiters;
   sj_status rc;
   if (timeout_s > 0 && !s->cv_done.wait_for(g, std::chrono::duration<double>(timeout_s), ready)) {
-    take_result(s, it->second, ticket, info, nullptr, 0);
+    take_result(s, t, ticket, info, nullptr, 0);
     rc = fail_fmt(SJ_ERR_TIMEOUT, "ticket %llu not finished after %.3f s", (unsigned long long)ticket, timeout_s);
   } else {
     if (timeout_s <= 0) s->cv_done.wait(g, ready);
-    rc = take_result(s, it->second, ticket, info, out, cap);
+    rc = take_result(s, t, ticket, info, out, cap);
   }
   --s->waiters;
   s->cv_done.notify_all();
