@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kBq) sjb_layout_kernel(const __grid_constant__
   __shared__ SjbStep st;
   __shared__ uint32_t s_err;
   __shared__ unsigned long long s_wsum[2], s_wact[2], s_wuse[2][SJ_MAX_DIMS];
-  __shared__ float s_wcost[2][SJ_MAX_DIMS];
+  __shared__ float s_cover[kBq], s_pcost[24];
   __shared__ long long s_wlo[2], s_whi[2];
   __shared__ uint32_t s_span[kBq], s_smax[2];
   __shared__ uint8_t s_pos[SJ_MAX_DIMS];
@@ -254,15 +254,8 @@ __global__ void __launch_bounds__(kBq) sjb_layout_kernel(const __grid_constant__
   }
   const unsigned long long wtot = __shfl_sync(kFull, incl, 31);
   const uint32_t ab = __ballot_sync(kFull, act);
-  float cost[SJ_MAX_DIMS];
   uint32_t ub[SJ_MAX_DIMS];
-  for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) {
-    const bool u = act && st.bm[q][d] != nullptr;
-    ub[d] = __ballot_sync(kFull, u);
-    float c = act ? (u ? st.sel[q][d] : 1.f) : 0.f;
-    for (uint32_t off = 16; off; off >>= 1) c += __shfl_xor_sync(kFull, c, off);
-    cost[d] = c;
-  }
+  for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) ub[d] = __ballot_sync(kFull, act && st.bm[q][d] != nullptr);
   long long lo = act ? sl.b : LLONG_MAX, hi = act ? sl.e : 0;
   for (uint32_t off = 16; off; off >>= 1) {
     lo = min(lo, __shfl_xor_sync(kFull, lo, off));
@@ -273,10 +266,7 @@ __global__ void __launch_bounds__(kBq) sjb_layout_kernel(const __grid_constant__
     s_wact[wp] = ab;
     s_wlo[wp] = lo;
     s_whi[wp] = hi;
-    for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) {
-      s_wuse[wp][d] = ub[d];
-      s_wcost[wp][d] = cost[d];
-    }
+    for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) s_wuse[wp][d] = ub[d];
   }
   __syncthreads();
   const unsigned long long total = s_wsum[0] + s_wsum[1];
@@ -290,21 +280,32 @@ __global__ void __launch_bounds__(kBq) sjb_layout_kernel(const __grid_constant__
     st.seg_b = active ? min(s_wlo[0], s_wlo[1]) : 0;
     st.seg_e = active ? max(s_whi[0], s_whi[1]) : 0;
     st.n_dims = S.n_dims;
-    float c[SJ_MAX_DIMS];
-    for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) {
-      st.use[d] = over ? 0ull : (s_wuse[0][d] | (s_wuse[1][d] << 32));
-      c[d] = s_wcost[0][d] + s_wcost[1][d];
-      st.order[d] = d;
-    }
-    for (uint32_t a = 1; a < S.n_dims; ++a)  // fewest expected surviving candidates first
-      for (uint32_t b = a; b > 0 && c[st.order[b]] < c[st.order[b - 1]]; --b) {
-        const uint32_t t = st.order[b];
-        st.order[b] = st.order[b - 1];
-        st.order[b - 1] = t;
-      }
-    for (uint32_t k = 0; k < S.n_dims; ++k) s_pos[st.order[k]] = (uint8_t)k;
+    for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) st.use[d] = over ? 0ull : (s_wuse[0][d] | (s_wuse[1][d] << 32));
     st.error = s_err;
     if (s_err) atomicOr(&ctr->error, s_err);
+  }
+  __syncthreads();
+  // lookup order: each of the first n! threads prices one order, thread 0 takes the cheapest
+  s_cover[q] = ((st.active >> q) & 1ull)
+                   ? (float)((double)(sl.e - sl.b) / (double)max(1ll, (long long)(st.seg_e - st.seg_b)))
+                   : 0.f;
+  __syncthreads();
+  uint32_t n_perm = 1;
+  for (uint32_t i = 2; i <= S.n_dims; ++i) n_perm *= i;
+  if (q < n_perm) {
+    uint32_t perm[SJ_MAX_DIMS];
+    sjb_perm_of(q, S.n_dims, perm);
+    s_pcost[q] = sjb_order_lookups(st, s_cover, perm, S.n_dims);
+  }
+  __syncthreads();
+  if (q == 0) {
+    uint32_t bi = 0;
+    for (uint32_t i = 1; i < n_perm; ++i)
+      if (s_pcost[i] < s_pcost[bi]) bi = i;
+    uint32_t perm[SJ_MAX_DIMS] = {0, 1, 2, 3};
+    sjb_perm_of(bi, S.n_dims, perm);
+    for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) st.order[d] = d < S.n_dims ? perm[d] : d;
+    for (uint32_t k = 0; k < S.n_dims; ++k) s_pos[st.order[k]] = (uint8_t)k;
   }
   const bool cand = a2 && sl.span <= 2048u;
   s_span[q] = cand ? sl.span : 0u;

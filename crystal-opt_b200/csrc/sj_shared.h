@@ -180,9 +180,56 @@ __host__ __device__ inline uint32_t sjb_group_layout(const SjbSchemaRt& S, const
   return err;
 }
 
-// Per-step fields: dimension use masks, lookup order (fewest expected surviving
-// candidates first), grouped-dimension positions and shared-memory partials
-// (smallest spans first, while they fit).
+// Dimension order number `idx` (0 <= idx < n!) by its factorial-base digits.
+__host__ __device__ inline void sjb_perm_of(uint32_t idx, uint32_t n, uint32_t* out) {
+  uint32_t pool[SJ_MAX_DIMS] = {0, 1, 2, 3};
+  uint32_t fact = 1;
+  for (uint32_t i = 2; i < n; ++i) fact *= i;
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t left = n - 1 - k;
+    const uint32_t r = left ? idx / fact : 0u;
+    if (left) idx %= fact;
+    out[k] = pool[r];
+    for (uint32_t j = r; j + 1 < n - k; ++j) pool[j] = pool[j + 1];
+    if (left > 1) fact /= left;
+  }
+}
+
+// Expected mask-word lookups per scanned row for a dimension order: position k
+// is looked up when some query still alive uses its dimension, and query q is
+// alive there with probability cover[q] (its share of the scanned rows) times
+// its selectivities on the dimensions before k.  Queries are taken as
+// independent of one another.
+__host__ __device__ inline float sjb_order_lookups(const SjbStep& st, const float* cover, const uint32_t* perm,
+                                                   uint32_t nd) {
+  float alive[kBq];
+  for (int q = 0; q < kBq; ++q) alive[q] = ((st.active >> q) & 1ull) ? cover[q] : 0.f;
+  float cost = 0.f;
+  for (uint32_t k = 0; k < nd; ++k) {
+    const uint32_t d = perm[k];
+    float none = 1.f;
+    for (int q = 0; q < kBq; ++q) {
+      if (!((st.use[d] >> q) & 1ull)) continue;
+      none *= 1.f - alive[q];
+      alive[q] *= st.sel[q][d];
+    }
+    cost += 1.f - none;
+  }
+  return cost;
+}
+
+// Share of the step's segment that each active slot's row range covers.
+__host__ __device__ inline void sjb_cover(const SjbStep& st, float* cover) {
+  const double seg = st.seg_e > st.seg_b ? (double)(st.seg_e - st.seg_b) : 1.0;
+  for (int q = 0; q < kBq; ++q) {
+    const SjbSlot& s = st.slot[q];
+    cover[q] = ((st.active >> q) & 1ull) ? (float)((double)(s.e - s.b) / seg) : 0.f;
+  }
+}
+
+// Per-step fields: dimension use masks, lookup order (fewest expected mask-word
+// lookups per row over every order), grouped-dimension positions and
+// shared-memory partials (smallest spans first, while they fit).
 __host__ __device__ inline void sjb_step_layout(SjbStep& st, uint32_t n_dims, uint32_t smem_capacity) {
   st.n_dims = n_dims;
   for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) st.use[d] = 0;
@@ -191,22 +238,21 @@ __host__ __device__ inline void sjb_step_layout(SjbStep& st, uint32_t n_dims, ui
     for (uint32_t d = 0; d < n_dims; ++d)
       if (st.bm[q][d]) st.use[d] |= 1ull << q;
   }
-  float cost[SJ_MAX_DIMS];
-  for (uint32_t d = 0; d < n_dims; ++d) {
-    float c = 0.f;
-    for (int q = 0; q < kBq; ++q) {
-      if (!((st.active >> q) & 1ull)) continue;
-      c += ((st.use[d] >> q) & 1ull) ? st.sel[q][d] : 1.f;
+  float cover[kBq];
+  sjb_cover(st, cover);
+  uint32_t n_perm = 1;
+  for (uint32_t i = 2; i <= n_dims; ++i) n_perm *= i;
+  float best = 3.4e38f;
+  for (uint32_t d = 0; d < SJ_MAX_DIMS; ++d) st.order[d] = d;
+  for (uint32_t i = 0; i < n_perm; ++i) {
+    uint32_t perm[SJ_MAX_DIMS];
+    sjb_perm_of(i, n_dims, perm);
+    const float c = sjb_order_lookups(st, cover, perm, n_dims);
+    if (c < best) {
+      best = c;
+      for (uint32_t k = 0; k < n_dims; ++k) st.order[k] = perm[k];
     }
-    cost[d] = c;
-    st.order[d] = d;
   }
-  for (uint32_t i = 1; i < n_dims; ++i)  // insertion sort, stable
-    for (uint32_t j = i; j > 0 && cost[st.order[j]] < cost[st.order[j - 1]]; --j) {
-      uint32_t t = st.order[j];
-      st.order[j] = st.order[j - 1];
-      st.order[j - 1] = t;
-    }
   uint8_t pos[SJ_MAX_DIMS] = {0, 0, 0, 0};
   for (uint32_t k = 0; k < n_dims; ++k) pos[st.order[k]] = (uint8_t)k;
   uint32_t used = 0;

@@ -243,7 +243,28 @@ static void test_layouts() {
   }
 }
 
+static void test_perms() {
+  for (uint32_t n = 1; n <= 4; ++n) {
+    uint32_t n_perm = 1;
+    for (uint32_t i = 2; i <= n; ++i) n_perm *= i;
+    std::vector<uint32_t> codes;
+    for (uint32_t i = 0; i < n_perm; ++i) {
+      uint32_t perm[SJ_MAX_DIMS];
+      sjb_perm_of(i, n, perm);
+      uint32_t seen = 0, code = 0;
+      for (uint32_t k = 0; k < n; ++k) {
+        CHECK(perm[k] < n && !((seen >> perm[k]) & 1u));
+        seen |= 1u << perm[k];
+        code = code * 4 + perm[k];
+      }
+      for (uint32_t c : codes) CHECK(c != code);
+      codes.push_back(code);
+    }
+  }
+}
+
 int main() {
+  test_perms();
   test_range_alloc();
   test_filter_cache();
   test_coverage();
