@@ -46,6 +46,7 @@ enum {
   SJ_COL_SUPP_SEL = 22,
   SJ_COL_PART_CATEGORY = 31,
   SJ_COL_PART_SEL = 32,
+  SJ_COL_PART_BRAND = 33,
   SJ_COL_DATE_SEL = 42
 };
 

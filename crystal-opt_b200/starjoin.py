@@ -39,7 +39,7 @@ PRED_ALL, PRED_IN, PRED_RANGE = 0, 1, 2
 COL_FK_CUST, COL_FK_SUPP, COL_FK_PART, COL_FK_DATE, COL_REVENUE, COL_SUPPLYCOST = 1, 2, 3, 4, 5, 6
 COL_CUST_CITY, COL_CUST_SEL = 11, 12
 COL_SUPP_CITY, COL_SUPP_SEL = 21, 22
-COL_PART_CATEGORY, COL_PART_SEL = 31, 32
+COL_PART_CATEGORY, COL_PART_SEL, COL_PART_BRAND = 31, 32, 33
 COL_DATE_SEL = 42
 GEN_UNIFORM, GEN_DATEKEY, GEN_SEQ, GEN_DATE_SEQ, GEN_DATE_YEAR = 0, 1, 2, 3, 4
 DATE_DAYS, DATE_MIN, DATE_MAX = 2556, 19920101, 19981230
@@ -209,37 +209,68 @@ class StarSchema:
                 "fk_part": (n, COL_FK_PART, GEN_UNIFORM, 1, self.part_rows),
                 "supplycost": (n, COL_SUPPLYCOST, GEN_UNIFORM, 1, 100_000),
                 "p_key": (self.part_rows, 0, GEN_SEQ, 1, 0),
-                "p_category": (self.part_rows, COL_PART_CATEGORY, GEN_UNIFORM, 0, 24),
+                "p_brand1": (self.part_rows, COL_PART_BRAND, GEN_UNIFORM, 0, 999),
                 "p_sel": (self.part_rows, COL_PART_SEL, GEN_UNIFORM, 0, 999),
             })
         return specs
+
+    def derived_specs(self) -> Dict[str, tuple]:
+        """name -> (base column, divisor): SSB's nested codes.  A city's nation is
+        city // 10 and its region nation // 5 (25 nations, 5 regions over 250
+        cities); a brand's category is brand // 40 and its manufacturer
+        category // 5 (1000 brands, 25 categories, 5 manufacturers)."""
+        d = {"c_nation": ("c_city", 10), "c_region": ("c_city", 50),
+             "s_nation": ("s_city", 10), "s_region": ("s_city", 50)}
+        if self.part_rows:
+            d.update({"p_category": ("p_brand1", 40), "p_mfgr": ("p_brand1", 200)})
+        return d
+
+    def column_names(self) -> List[str]:
+        return list(self.column_specs()) + list(self.derived_specs())
+
+
+def _wanted(schema: StarSchema, names: Optional[Sequence[str]]):
+    """Base columns to generate and derived columns to compute for `names`."""
+    derived = schema.derived_specs()
+    want = set(schema.column_names()) if names is None else set(names)
+    bases = {n for n in want if n in schema.column_specs()}
+    bases |= {derived[n][0] for n in want if n in derived}
+    return bases, [n for n in derived if n in want], want
 
 
 def gen_host(schema: StarSchema, names: Optional[Sequence[str]] = None, threads: int = 0) -> Dict[str, np.ndarray]:
     """Generate columns on the host (no GPU needed)."""
     lib = load()
+    bases, derived, want = _wanted(schema, names)
     out = {}
     for name, (n, col, kind, lo, hi) in schema.column_specs().items():
-        if names is not None and name not in names:
+        if name not in bases:
             continue
         a = np.empty(max(n, 0), dtype=np.int32)
         lib.sj_gen_column_host(a.ctypes.data, n, schema.seed, col, kind, lo, hi, threads)
         out[name] = a
-    return out
+    for name in derived:
+        base, div = schema.derived_specs()[name]
+        out[name] = (out[base] // div).astype(np.int32)
+    return {k: v for k, v in out.items() if k in want}
 
 
 def gen_device(schema: StarSchema, names: Optional[Sequence[str]] = None, device: int = 0):
     """Generate columns directly into torch CUDA tensors (same values as gen_host)."""
     import torch
     lib = load()
+    bases, derived, want = _wanted(schema, names)
     out = {}
     for name, (n, col, kind, lo, hi) in schema.column_specs().items():
-        if names is not None and name not in names:
+        if name not in bases:
             continue
         t = torch.empty(max(n, 1), dtype=torch.int32, device=f"cuda:{device}")[:n]
         check(lib.sj_gen_column_device(t.data_ptr(), n, schema.seed, col, kind, lo, hi, None))
         out[name] = t
-    return out
+    for name in derived:
+        base, div = schema.derived_specs()[name]
+        out[name] = torch.div(out[base], div, rounding_mode="floor").to(torch.int32).contiguous()
+    return {k: v for k, v in out.items() if k in want}
 
 
 # ------------------------------------------------------------------ queries ----
@@ -266,6 +297,59 @@ def q33_query(schema: StarSchema, order=(0, 1, 2), lip=True, bf_bits_per_key=0, 
         "order": list(order), "lip": bool(lip), "adaptive": bool(adaptive),
         "bf_bits_per_key": int(bf_bits_per_key), "bf_hashes": int(bf_hashes),
     }
+
+
+def _dim(fk, key, attr, pred, payload=None, prange=(0, 0), ht_len=0, key_min=0):
+    return {"fk": fk, "key": key, "attr": attr, "payload": payload, "key_min": key_min, "ht_len": ht_len,
+            "pred": pred, "group": payload is not None, "payload_range": prange}
+
+
+def _date_dim(pred=("all",)):
+    return _dim("fk_date", "d_key", "d_year" if pred[0] != "all" else None, pred, "d_year", (1992, 1998),
+                DATE_MAX - DATE_MIN + 1, DATE_MIN)
+
+
+def _shape(dims, schema, order, lip, bpk, k, adaptive, sub=None):
+    return {"dims": dims, "measure": "revenue", "measure_sub": sub, "row_range": (0, schema.fact_rows),
+            "order": list(order), "lip": bool(lip), "adaptive": bool(adaptive), "bf_bits_per_key": int(bpk),
+            "bf_hashes": int(k)}
+
+
+def q21_query(schema: StarSchema, order=(0, 1, 2), lip=True, bf_bits_per_key=0, bf_hashes=2,
+              adaptive=False) -> Dict[str, Any]:
+    """SSB Q2.1 as src/ssb-jo/q21/0-lip.cu runs it: dims 0 = supplier (s_region == 1,
+    key-only table: BlockBuildSelectivePHT_1), 1 = part (p_category == 1, payload
+    p_brand1), 2 = date (every day, payload d_year); group by (p_brand1, d_year);
+    SUM(revenue).  Result tuples: (p_brand1, d_year, count, sum)."""
+    dims = [_dim("fk_supp", "s_key", "s_region", ("in", [1]), ht_len=schema.supp_rows),
+            _dim("fk_part", "p_key", "p_category", ("in", [1]), "p_brand1", (0, 999), schema.part_rows),
+            _date_dim()]
+    return _shape(dims, schema, order, lip, bf_bits_per_key, bf_hashes, adaptive)
+
+
+def q31_query(schema: StarSchema, order=(0, 1, 2), lip=True, bf_bits_per_key=0, bf_hashes=2,
+              adaptive=False) -> Dict[str, Any]:
+    """SSB Q3.1 as src/ssb-jo/q31/0-lip.cu runs it: dims 0 = customer (c_region == 2,
+    payload c_nation), 1 = supplier (s_region == 2, payload s_nation), 2 = date
+    (1992 <= d_year <= 1997); group by (c_nation, s_nation, d_year); SUM(revenue).
+    Result tuples: (c_nation, s_nation, d_year, count, sum)."""
+    dims = [_dim("fk_cust", "c_key", "c_region", ("in", [2]), "c_nation", (0, 24), schema.cust_rows),
+            _dim("fk_supp", "s_key", "s_region", ("in", [2]), "s_nation", (0, 24), schema.supp_rows),
+            _date_dim(("range", 1992, 1997))]
+    return _shape(dims, schema, order, lip, bf_bits_per_key, bf_hashes, adaptive)
+
+
+def q41_query(schema: StarSchema, order=(0, 1, 2, 3), lip=True, bf_bits_per_key=0, bf_hashes=2,
+              adaptive=False) -> Dict[str, Any]:
+    """SSB Q4.1 as src/ssb-jo/q41/0-lip.cu runs it: dims 0 = supplier (s_region == 1,
+    key-only), 1 = customer (c_region == 1, payload c_nation), 2 = part (p_mfgr IN
+    {0, 1}, key-only), 3 = date (every day, payload d_year); group by (c_nation,
+    d_year); SUM(revenue - supplycost).  Result tuples: (c_nation, d_year, count, sum)."""
+    dims = [_dim("fk_supp", "s_key", "s_region", ("in", [1]), ht_len=schema.supp_rows),
+            _dim("fk_cust", "c_key", "c_region", ("in", [1]), "c_nation", (0, 24), schema.cust_rows),
+            _dim("fk_part", "p_key", "p_mfgr", ("in", [0, 1]), ht_len=schema.part_rows),
+            _date_dim()]
+    return _shape(dims, schema, order, lip, bf_bits_per_key, bf_hashes, adaptive, sub="supplycost")
 
 
 def fill_plan(query: Dict[str, Any], cols: Dict[str, Any], fact_rows: int, tune: Optional[dict] = None):

@@ -1,9 +1,10 @@
-"""Compile the reference's own SSB Q3.3 drivers into oracle/_ref/ -- TEST INFRASTRUCTURE.
+"""Compile the reference's own SSB drivers into oracle/_ref/ -- TEST INFRASTRUCTURE.
 
 The driver sources are compiled where they lie under the reference tree
 (default /root/reference, override with CRYSTAL_OPT_REF); nothing is copied.
-Each binary is one driver (src/ssb-jo/q33/<order>-<lip|naive>.cu) wrapped by
-ref_runner.cu, which supplies main() and the synthetic columns.  The reference's
+Each binary is one driver -- src/ssb-jo/q33/<order>-<lip|naive>.cu wrapped by
+ref_runner.cu, or src/ssb-jo/q{21,31,41}/0-lip.cu wrapped by ref_runner_shapes.cu --
+the wrapper supplying main() and the synthetic columns.  The reference's
 CUB 1.6.4 test header is replaced by ref_shim/cub/test/test_util.h.  Flags follow
 the reference Makefile (-O3 -lineinfo -Xptxas -dlcm=ca, Makefile:23,35) with the
 architecture switched to sm_100a.
@@ -47,15 +48,56 @@ def _compile(order: int, method: str) -> str:
     return out
 
 
+SHAPES = (21, 31, 41)  # src/ssb-jo/q21, q31, q41: order-0 LIP drivers
+
+
+def shape_binary(query: int) -> str:
+    return os.path.join(OUT, f"q{query}_0_lip")
+
+
+def _compile_shape(query: int) -> str:
+    src = os.path.join(REF, "src", "ssb-jo", f"q{query}", "0-lip.cu")
+    out = shape_binary(query)
+    runner = os.path.join(HERE, "ref_runner_shapes.cu")
+    deps = [src, runner, os.path.join(HERE, "ref_shim", "cub", "test", "test_util.h")]
+    if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
+        return out
+    cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+           "-Xptxas", "-dlcm=ca", "-I", REF, "-I", os.path.join(HERE, "ref_shim"),
+           f'-DREF_DRIVER="{src}"', f"-DREF_QUERY={query}", "-o", out + ".tmp", runner]
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
+    os.replace(out + ".tmp", out)
+    return out
+
+
 def build(jobs: int = 0) -> list[str]:
-    """Build all 12 drivers (skipped when the reference tree is absent)."""
+    """Build the 12 Q3.3 drivers and the Q2.1 / Q3.1 / Q4.1 LIP drivers
+    (skipped when the reference tree is absent)."""
     if not available():
         return []
     os.makedirs(OUT, exist_ok=True)
     jobs = jobs or min(8, os.cpu_count() or 1)
     with cf.ThreadPoolExecutor(jobs) as ex:
         futs = [ex.submit(_compile, o, m) for o in ORDERS for m in METHODS]
+        futs += [ex.submit(_compile_shape, q) for q in SHAPES]
         return [f.result() for f in futs]
+
+
+def parse_groups(text: str, width: int) -> list:
+    """Group lines of a shape driver's output: `width` integers per line after
+    the first "Result:" (other lines, e.g. "Num Matched ...", are skipped)."""
+    groups, on = [], False
+    for line in text.splitlines():
+        line = line.strip()
+        if line == "Result:":
+            on = True
+            continue
+        if line.startswith("Res Count:"):
+            break
+        parts = line.split()
+        if on and len(parts) == width and all(p.lstrip("-").isdigit() for p in parts):
+            groups.append(tuple(int(p) for p in parts))
+    return sorted(groups)
 
 
 def parse_output(text: str) -> dict:

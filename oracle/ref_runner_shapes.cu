@@ -1,0 +1,115 @@
+// ref_runner_shapes.cu -- TEST INFRASTRUCTURE: a main() around one of the
+// reference's own SSB Q2.1 / Q3.1 / Q4.1 LIP drivers (src/ssb-jo/q{21,31,41}/0-lip.cu),
+// compiled unmodified from its source tree by build_ref.py into oracle/_ref/.
+// It feeds the driver the seeded synthetic columns the engine's tests use (SSB's
+// nested codes derived as nation = city / 10, region = city / 50,
+// category = brand / 40, mfgr = brand / 200) and calls the driver's own
+// runQuery(), which prints one line per group.  REF_QUERY selects the driver.
+#define main crystal_reference_driver_main
+#include REF_DRIVER
+#undef main
+
+#include <thread>
+#include <vector>
+
+#include "../crystal-opt_b200/csrc/sj_datagen.h"
+
+static std::vector<int> ref_gen_host(long long n, unsigned long long seed, int col, int kind, int lo, int hi) {
+  std::vector<int> h((size_t)(n > 0 ? n : 1));
+  const uint64_t key = sj_stream_key(seed, (uint32_t)col);
+  unsigned nt = std::thread::hardware_concurrency();
+  if (nt == 0) nt = 1;
+  if (nt > 64) nt = 64;
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < nt; ++t)
+    pool.emplace_back([&, t]() {
+      for (long long i = n * t / nt; i < n * (t + 1) / nt; ++i) h[i] = sj_gen_value(key, kind, lo, hi, (uint64_t)i);
+    });
+  for (auto& th : pool) th.join();
+  return h;
+}
+
+static std::vector<int> div_by(const std::vector<int>& v, int d) {
+  std::vector<int> out(v.size());
+  for (size_t i = 0; i < v.size(); ++i) out[i] = v[i] / d;
+  return out;
+}
+
+static int* to_gpu(std::vector<int>& h, long long n) { return loadToGPU<int>(h.data(), (int)n, g_allocator); }
+
+int main(int argc, char** argv) {
+  CommandLineArgs args(argc, argv);
+  unsigned long long seed = 1;
+  int n = 6000000, c_len = 30000, s_len = 2000, p_len = 200000;
+  args.GetCmdLineArgument("seed", seed);
+  args.GetCmdLineArgument("n", n);
+  args.GetCmdLineArgument("c", c_len);
+  args.GetCmdLineArgument("s", s_len);
+  args.GetCmdLineArgument("p", p_len);
+  CubDebugExit(args.DeviceInit());
+  const int d_len = SJ_DATE_DAYS;
+
+  auto h_lo_orderdate = ref_gen_host(n, seed, SJ_COL_FK_DATE, SJ_GEN_DATEKEY, 0, 0);
+  auto h_lo_custkey = ref_gen_host(n, seed, SJ_COL_FK_CUST, SJ_GEN_UNIFORM, 1, c_len);
+  auto h_lo_suppkey = ref_gen_host(n, seed, SJ_COL_FK_SUPP, SJ_GEN_UNIFORM, 1, s_len);
+  auto h_lo_partkey = ref_gen_host(n, seed, SJ_COL_FK_PART, SJ_GEN_UNIFORM, 1, p_len);
+  auto h_lo_revenue = ref_gen_host(n, seed, SJ_COL_REVENUE, SJ_GEN_UNIFORM, 1, 10000000);
+  auto h_lo_supplycost = ref_gen_host(n, seed, SJ_COL_SUPPLYCOST, SJ_GEN_UNIFORM, 1, 100000);
+  auto h_d_datekey = ref_gen_host(d_len, seed, 0, SJ_GEN_DATE_SEQ, 0, 0);
+  auto h_d_year = ref_gen_host(d_len, seed, 0, SJ_GEN_DATE_YEAR, 0, 0);
+  auto h_s_suppkey = ref_gen_host(s_len, seed, 0, SJ_GEN_SEQ, 1, 0);
+  auto h_s_city = ref_gen_host(s_len, seed, SJ_COL_SUPP_CITY, SJ_GEN_UNIFORM, 0, 249);
+  auto h_c_custkey = ref_gen_host(c_len, seed, 0, SJ_GEN_SEQ, 1, 0);
+  auto h_c_city = ref_gen_host(c_len, seed, SJ_COL_CUST_CITY, SJ_GEN_UNIFORM, 0, 249);
+  auto h_p_partkey = ref_gen_host(p_len, seed, 0, SJ_GEN_SEQ, 1, 0);
+  auto h_p_brand1 = ref_gen_host(p_len, seed, SJ_COL_PART_BRAND, SJ_GEN_UNIFORM, 0, 999);
+  auto h_s_nation = div_by(h_s_city, 10), h_s_region = div_by(h_s_city, 50);
+  auto h_c_nation = div_by(h_c_city, 10), h_c_region = div_by(h_c_city, 50);
+  auto h_p_category = div_by(h_p_brand1, 40), h_p_mfgr = div_by(h_p_brand1, 200);
+
+  int* lo_orderdate = to_gpu(h_lo_orderdate, n);
+  int* lo_suppkey = to_gpu(h_lo_suppkey, n);
+  int* lo_revenue = to_gpu(h_lo_revenue, n);
+  int* d_datekey = to_gpu(h_d_datekey, d_len);
+  int* d_year = to_gpu(h_d_year, d_len);
+  int* s_suppkey = to_gpu(h_s_suppkey, s_len);
+  int* s_region = to_gpu(h_s_region, s_len);
+  printf("Result:\n");
+#if REF_QUERY == 21
+  int* lo_partkey = to_gpu(h_lo_partkey, n);
+  int* p_partkey = to_gpu(h_p_partkey, p_len);
+  int* p_brand1 = to_gpu(h_p_brand1, p_len);
+  int* p_category = to_gpu(h_p_category, p_len);
+  CubDebugExit(cudaDeviceSynchronize());
+  fflush(stdout);
+  runQuery(lo_orderdate, lo_partkey, lo_suppkey, lo_revenue, n, p_partkey, p_brand1, p_category, p_len, d_datekey,
+           d_year, d_len, s_suppkey, s_region, s_len, g_allocator);
+#elif REF_QUERY == 31
+  int* lo_custkey = to_gpu(h_lo_custkey, n);
+  int* s_nation = to_gpu(h_s_nation, s_len);
+  int* c_custkey = to_gpu(h_c_custkey, c_len);
+  int* c_region = to_gpu(h_c_region, c_len);
+  int* c_nation = to_gpu(h_c_nation, c_len);
+  CubDebugExit(cudaDeviceSynchronize());
+  fflush(stdout);
+  runQuery(lo_orderdate, lo_custkey, lo_suppkey, lo_revenue, n, d_datekey, d_year, d_len, s_suppkey, s_region,
+           s_nation, s_len, c_custkey, c_region, c_nation, c_len, g_allocator);
+#elif REF_QUERY == 41
+  int* lo_custkey = to_gpu(h_lo_custkey, n);
+  int* lo_partkey = to_gpu(h_lo_partkey, n);
+  int* lo_supplycost = to_gpu(h_lo_supplycost, n);
+  int* p_partkey = to_gpu(h_p_partkey, p_len);
+  int* p_mfgr = to_gpu(h_p_mfgr, p_len);
+  int* c_custkey = to_gpu(h_c_custkey, c_len);
+  int* c_region = to_gpu(h_c_region, c_len);
+  int* c_nation = to_gpu(h_c_nation, c_len);
+  CubDebugExit(cudaDeviceSynchronize());
+  fflush(stdout);
+  runQuery(lo_orderdate, lo_custkey, lo_partkey, lo_suppkey, lo_revenue, lo_supplycost, n, d_datekey, d_year, d_len,
+           p_partkey, p_mfgr, p_len, s_suppkey, s_region, s_len, c_custkey, c_region, c_nation, c_len, g_allocator);
+#else
+#error "REF_QUERY must be 21, 31 or 41"
+#endif
+  fflush(stdout);
+  return 0;
+}

@@ -1,5 +1,6 @@
-"""Build the reference's own SSB Q3.3 drivers against this repository's
-crystal/*.cuh device functions (the drop-in check).
+"""Build the reference's own SSB drivers (the 12 Q3.3 drivers and the Q2.1 /
+Q3.1 / Q4.1 LIP drivers) against this repository's crystal/*.cuh device
+functions (the drop-in check).
 
 Each driver (src/ssb-jo/q33/<order>-<lip|naive>.cu, compiled where it lies in
 the reference tree, default /root/reference or $CRYSTAL_OPT_REF) includes
@@ -49,6 +50,33 @@ def _compile(order: int, method: str) -> str:
     return out
 
 
+SHAPES = (21, 31, 41)
+
+
+def shape_binary(query: int) -> str:
+    return os.path.join(OUT, f"q{query}_0_lip")
+
+
+def _compile_shape(query: int) -> str:
+    """src/ssb-jo/q<query>/0-lip.cu against crystal/*.cuh, main() from oracle/ref_runner_shapes.cu."""
+    src = os.path.join(REF, "src", "ssb-jo", f"q{query}", "0-lip.cu")
+    out = shape_binary(query)
+    runner = os.path.join(ROOT, "oracle", "ref_runner_shapes.cu")
+    hdrs = [os.path.join(ROOT, "crystal-opt_b200", "crystal", f) for f in os.listdir(
+        os.path.join(ROOT, "crystal-opt_b200", "crystal"))]
+    deps = [src, runner] + hdrs
+    if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
+        return out
+    cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+           "-I", os.path.join(ROOT, "crystal-opt_b200"), "-I", os.path.join(ROOT, "oracle", "ref_shim"),
+           f'-DREF_DRIVER="{src}"', f"-DREF_QUERY={query}", "-o", out + ".tmp", runner]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"{src}: {r.stderr[-2000:]}")
+    os.replace(out + ".tmp", out)
+    return out
+
+
 def build(jobs: int = 0) -> list[str]:
     if not available():
         return []
@@ -56,6 +84,7 @@ def build(jobs: int = 0) -> list[str]:
     jobs = jobs or min(8, os.cpu_count() or 1)
     with cf.ThreadPoolExecutor(jobs) as ex:
         futs = [ex.submit(_compile, o, m) for o in range(6) for m in ("lip", "naive")]
+        futs += [ex.submit(_compile_shape, q) for q in SHAPES]
         return [f.result() for f in futs]
 
 

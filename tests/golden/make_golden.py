@@ -5,7 +5,8 @@ src/ssb-jo/q33/*.cu drivers, built by oracle/build_ref.py) on the seeded small
 star schema and records the groups each prints: (d_year, c_city, s_city, int32
 SUM(lo_revenue)).  Needs a GPU; run from the repository root:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # Q3.3, all 12 drivers
+    python tests/golden/make_golden.py --shapes   # Q2.1 / Q3.1 / Q4.1
 """
 import json
 import os
@@ -29,6 +30,29 @@ def run_driver(order: int, method: str, schema, trials: int = 1, probe_trials: i
     return build_ref.parse_output(out)
 
 
+def shapes():
+    """Groups printed by the reference's Q2.1 / Q3.1 / Q4.1 LIP drivers
+    (oracle/_ref/q{21,31,41}_0_lip) on the seeded SF1-sized schema."""
+    from workloads import SHAPES_SMALL, SHAPE_WIDTH
+    sc = SHAPES_SMALL
+    rec = {"what": "groups printed by the reference's src/ssb-jo/q{21,31,41}/0-lip.cu drivers on the seeded "
+                   "schema; columns as each driver prints them",
+           "schema": {"seed": sc.seed, "fact_rows": sc.fact_rows, "cust_rows": sc.cust_rows,
+                      "supp_rows": sc.supp_rows, "part_rows": sc.part_rows},
+           "columns": {"21": ["d_year", "p_brand1", "sum_u64"], "31": ["d_year", "c_nation", "s_nation", "sum_u64"],
+                       "41": ["d_year", "c_nation", "sum_u64(revenue-supplycost)"]},
+           "groups": {}}
+    for q in build_ref.SHAPES:
+        cmd = [build_ref.shape_binary(q), f"--seed={sc.seed}", f"--n={sc.fact_rows}", f"--c={sc.cust_rows}",
+               f"--s={sc.supp_rows}", f"--p={sc.part_rows}"]
+        out = subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=600).stdout
+        rec["groups"][str(q)] = build_ref.parse_groups(out, SHAPE_WIDTH[q])
+    path = os.path.join(ROOT, "tests", "golden", "shapes_small_reference.json")
+    with open(path, "w") as f:
+        json.dump(rec, f, indent=1)
+    print(path, {q: len(v) for q, v in rec["groups"].items()})
+
+
 def main():
     drivers = {}
     for o in range(6):
@@ -50,4 +74,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if "--shapes" in sys.argv:
+        shapes()
+    else:
+        main()

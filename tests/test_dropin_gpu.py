@@ -34,3 +34,26 @@ def test_reference_driver_on_b200_device_api(sj, oracle, torch_cuda, order, meth
     assert got == want
     with open(GOLDEN) as f:
         assert got == sorted(tuple(r) for r in json.load(f)["groups"])
+
+
+@pytest.mark.parametrize("query", [21, 31, 41])
+def test_reference_shape_driver_on_b200_device_api(sj, oracle, torch_cuda, query):
+    """The reference's own Q2.1 / Q3.1 / Q4.1 LIP drivers, compiled unmodified
+    against crystal/*.cuh, print the oracle's groups and the golden vectors of
+    the same drivers built against the reference's headers."""
+    from workloads import SHAPE_QUERIES, SHAPE_WIDTH, SHAPES_SMALL, shape_as_printed
+    exe = dropin_build.shape_binary(query)
+    if not os.path.exists(exe):
+        pytest.skip("drop-in drivers not built")
+    import build_ref
+    sc = SHAPES_SMALL
+    out = subprocess.run([exe, f"--seed={sc.seed}", f"--n={sc.fact_rows}", f"--c={sc.cust_rows}",
+                          f"--s={sc.supp_rows}", f"--p={sc.part_rows}"],
+                         check=True, capture_output=True, text=True, timeout=300).stdout
+    got = build_ref.parse_groups(out, SHAPE_WIDTH[query])
+    want = shape_as_printed(query, oracle.run(SHAPE_QUERIES[query](sc), sj.gen_host(sc)))
+    assert got == want
+    golden = os.path.join(os.path.dirname(__file__), "golden", "shapes_small_reference.json")
+    if os.path.exists(golden):
+        with open(golden) as f:
+            assert got == [tuple(r) for r in json.load(f)["groups"][str(query)]]

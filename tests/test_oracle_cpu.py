@@ -123,3 +123,19 @@ def test_oracle_matches_reference_cuda_golden(sj, oracle):
     assert got == want
     for drv in g["drivers"].values():
         assert sorted(tuple(r) for r in drv) == want  # every order, LIP and naive agree
+
+
+def test_oracle_matches_reference_shape_golden(sj, oracle):
+    """Pins the oracle on the other query shapes: groups printed by the
+    reference's own Q2.1 / Q3.1 / Q4.1 LIP drivers (oracle/_ref, run on a B200)
+    on the seeded SF1-sized schema; their sums are uint64 (Q4.1: revenue -
+    supplycost, two's complement)."""
+    from workloads import SHAPE_QUERIES, shape_as_printed
+    g = _golden("shapes_small_reference.json")
+    sc = sj.StarSchema(**g["schema"])
+    cols = sj.gen_host(sc)
+    for q, make in SHAPE_QUERIES.items():
+        want = sorted(tuple(r) for r in g["groups"][str(q)])
+        assert want, q
+        got = shape_as_printed(q, oracle.run(make(sc), cols))
+        assert got == [tuple(w) for w in want], q

@@ -22,6 +22,24 @@ REF_DRIVER_ORDERS = {
 
 SMALL = sj.StarSchema(seed=0x5EED0001, fact_rows=6_000_000, cust_rows=30_000, supp_rows=2_000)
 FULL = sj.StarSchema(seed=0x5EED0002, fact_rows=120_000_000, cust_rows=600_000, supp_rows=40_000)
+# SSB scale-factor-1 dimension sizes for the Q2.1 / Q3.1 / Q4.1 shapes
+SHAPES_SMALL = sj.StarSchema(seed=0x5EED0009, fact_rows=6_000_000, cust_rows=30_000, supp_rows=2_000,
+                             part_rows=200_000)
+SHAPE_QUERIES = {21: sj.q21_query, 31: sj.q31_query, 41: sj.q41_query}
+SHAPE_WIDTH = {21: 3, 31: 4, 41: 3}  # integers per group line the reference drivers print
+
+
+def shape_as_printed(query: int, rows: List[tuple]) -> List[tuple]:
+    """Engine / oracle result tuples in the order the reference drivers print
+    them: Q2.1 (d_year, p_brand1, sum), Q3.1 (d_year, c_nation, s_nation, sum),
+    Q4.1 (d_year, c_nation, sum) -- src/ssb-jo/q{21,31,41}/0-lip.cu result loops."""
+    if query == 21:
+        return sorted((y, b, v) for (b, y, c, v) in rows)
+    if query == 31:
+        return sorted((y, cn, sn, v) for (cn, sn, y, c, v) in rows)
+    return sorted((y, cn, v) for (cn, y, c, v) in rows)
+
+
 FOURDIM = sj.StarSchema(seed=0x5EED0003, fact_rows=120_000_000, cust_rows=600_000, supp_rows=40_000,
                         part_rows=1_000_000)
 
