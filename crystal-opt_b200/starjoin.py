@@ -149,6 +149,9 @@ def load(build_if_missing: bool = True) -> C.CDLL:
                                     C.POINTER(C.c_int64), P]),
         "sj_noalloc_last_error": (C.c_char_p, []),
         "sj_autotune": (C.c_int, [P, C.POINTER(SjPlan), C.POINTER(SjAutotuneOpts), C.POINTER(SjAutotuneReport), P]),
+        "sj_ssb_column_file": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64]),
+        "sj_ssb_load_column": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64, P]),
+        "sj_ssb_store_column": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -166,6 +169,7 @@ def exported_symbols() -> List[str]:
         "sj_query_fetch", "sj_query_get_stats", "sj_query_release", "sj_run_plain",
         "sj_ssb_q33_run", "sj_bloom_test", "sj_gen_column_device", "sj_gen_column_host",
         "sj_ssb_q33_run_noalloc", "sj_noalloc_last_error", "sj_autotune",
+        "sj_ssb_column_file", "sj_ssb_load_column", "sj_ssb_store_column",
     ]
 
 
@@ -271,6 +275,40 @@ def gen_device(schema: StarSchema, names: Optional[Sequence[str]] = None, device
         base, div = schema.derived_specs()[name]
         out[name] = torch.div(out[base], div, rounding_mode="floor").to(torch.int32).contiguous()
     return {k: v for k, v in out.items() if k in want}
+
+
+# ------------------------------------------------------------- SSB files ----
+# Engine column names -> SSB column names (the reference's file layout).
+SSB_NAMES = {"fk_cust": "lo_custkey", "fk_supp": "lo_suppkey", "fk_part": "lo_partkey", "fk_date": "lo_orderdate",
+             "revenue": "lo_revenue", "supplycost": "lo_supplycost", "c_key": "c_custkey", "c_city": "c_city",
+             "c_nation": "c_nation", "c_region": "c_region", "s_key": "s_suppkey", "s_city": "s_city",
+             "s_nation": "s_nation", "s_region": "s_region", "p_key": "p_partkey", "p_brand1": "p_brand1",
+             "p_category": "p_category", "p_mfgr": "p_mfgr", "d_key": "d_datekey", "d_year": "d_year"}
+
+
+def ssb_file_name(column: str) -> str:
+    buf = C.create_string_buffer(64)
+    check(load().sj_ssb_column_file(column.encode(), buf, 64))
+    return buf.value.decode()
+
+
+def store_ssb_columns(directory: str, cols: Dict[str, np.ndarray]) -> None:
+    """Write host columns (engine names) as the reference's column files."""
+    for name, a in cols.items():
+        if name not in SSB_NAMES:
+            continue
+        a = np.ascontiguousarray(a, dtype=np.int32)
+        check(load().sj_ssb_store_column(directory.encode(), SSB_NAMES[name].encode(), a.size, a.ctypes.data))
+
+
+def load_ssb_columns(directory: str, lengths: Dict[str, int]) -> Dict[str, np.ndarray]:
+    """Read the reference's column files: engine name -> number of values."""
+    out = {}
+    for name, n in lengths.items():
+        a = np.empty(max(n, 1), dtype=np.int32)[:n]
+        check(load().sj_ssb_load_column(directory.encode(), SSB_NAMES[name].encode(), n, a.ctypes.data))
+        out[name] = a
+    return out
 
 
 # ------------------------------------------------------------------ queries ----

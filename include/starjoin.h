@@ -256,6 +256,19 @@ sj_status sj_bloom_test(const int32_t* keys, const int32_t* flags, int64_t n_key
                         int32_t bits_per_key, int32_t hashes, int32_t key_min,
                         int32_t direct_words, void* stream);
 
+/* ---- the reference's column files (src/ssb/ssb_utils.h:106-171) ----------
+ * One headerless file of native little-endian int32 values per SSB column,
+ * named by table and by the column's position in SSB's column list
+ * ("lo_custkey" -> "LINEORDER2", "d_year" -> "DDATE4").  With these, SSB data
+ * in the reference's data directory loads into the engine, and synthetic
+ * columns can be written for the reference's own drivers to read. */
+/* The file name of an SSB column (NUL-terminated into out[cap]). */
+sj_status sj_ssb_column_file(const char* column, char* out, int64_t cap);
+/* Read n values of `column` from directory dir into host memory. */
+sj_status sj_ssb_load_column(const char* dir, const char* column, int64_t n, int32_t* out);
+/* Write n host values as `column`'s file in directory dir. */
+sj_status sj_ssb_store_column(const char* dir, const char* column, int64_t n, const int32_t* data);
+
 /* ---- synthetic data on the device (same values as the host generator) ---- */
 /* Fill dst[0..n) with generated column values (see sj_datagen.h kinds). */
 sj_status sj_gen_column_device(int32_t* dst, int64_t n, uint64_t seed, int32_t col,
