@@ -12,6 +12,13 @@
 //
 // `plain = 1` serves the same requests one at a time through the plain engine
 // (sj_run_plain), the baseline the shared form is measured against.
+// `solo_plain = 1` sends a query that finds the scan idle and no other query
+// waiting through the plain engine too, when its row range fits in one scan
+// step: alone, the plain probe reads only the fact columns its survivors need
+// (the shared scan reads every column over the query's range), so a short
+// query's latency is the plain engine's.  A longer query still starts the
+// shared scan, which later arrivals join at the next step instead of queueing
+// behind it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -530,14 +537,16 @@ bool complete_step(sjs_server* s, int b) {
   return true;
 }
 
-void plain_one(sjs_server* s, uint64_t id) {
+// Run ticket `id` (the queue's head) through the plain engine; false if it was
+// cancelled before it started.
+bool plain_one(sjs_server* s, uint64_t id) {
   SjNvtxRange nvtx_range("sjs.plain_query");
   QueryCopy qc;
   {
     std::lock_guard<std::mutex> g(s->mu);
-    if (s->pending.empty() || s->pending.front() != id) return;  // cancelled meanwhile
+    if (s->pending.empty() || s->pending.front() != id) return false;  // cancelled meanwhile
     s->pending.pop_front();
-    if (!pending_query(s, id, qc)) return;
+    if (!pending_query(s, id, qc)) return false;
     s->tickets[id].admit_s = now_s();
     ++s->stats.admitted;
   }
@@ -585,6 +594,11 @@ void plain_one(sjs_server* s, uint64_t id) {
     rc = sj_run_plain(s->eng, &plan, 0, rows.data(), (int64_t)rows.size(), &n, &ms, s->st);
   }
   std::vector<sjb_row> out;
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->tickets.find(id);
+    if (rc == SJ_OK && it != s->tickets.end() && it->second.cancel) rc = SJ_ERR_CANCELLED;
+  }
   if (rc == SJ_OK) {
     out.resize((size_t)n);
     for (int64_t i = 0; i < n; ++i) {
@@ -599,6 +613,38 @@ void plain_one(sjs_server* s, uint64_t id) {
     ++s->stats.steps;
   }
   finish_ticket(s, id, rc, std::move(out));
+  return true;
+}
+
+// Whether the plain engine can answer q: its group space (full ranges of the
+// grouped attributes, as plain_one lays it out) within the plain engine's limits.
+bool plain_fits(const sjs_server* s, const sjb_query& q) {
+  uint64_t groups = 1;
+  for (int k = 0; k < q.n_preds; ++k) {
+    const sjb_pred& p = q.preds[k];
+    if (p.group_attr < 0) continue;
+    const int64_t span = s->S.attr_max[p.dim][p.group_attr] - s->S.attr_min[p.dim][p.group_attr] + 1;
+    if (span < 1 || span > SJ_MAX_PAYLOAD_SPAN) return false;
+    groups *= (uint64_t)span;
+    if (groups > (1ull << 26)) return false;
+  }
+  return true;
+}
+
+// The one waiting query when the scan is idle, nothing else waits and its row
+// range fits in one scan step (0 otherwise).
+uint64_t solo_candidate(sjs_server* s) {
+  if (!s->cfg.solo_plain || s->rec[0].valid || s->rec[1].valid) return 0;
+  for (const Slot& sl : s->slots)
+    if (sl.used) return 0;
+  std::lock_guard<std::mutex> g(s->mu);
+  if (s->pending.size() != 1) return 0;
+  const uint64_t id = s->pending.front();
+  auto it = s->tickets.find(id);
+  if (it == s->tickets.end() || it->second.done) return 0;
+  const sjb_query& q = it->second.q;
+  if (q.row_end - q.row_begin > s->step_rows || !plain_fits(s, q)) return 0;
+  return id;
 }
 
 void loop(sjs_server* s) {
@@ -614,6 +660,7 @@ void loop(sjs_server* s) {
     }
     const double t0 = now_s();
     bool ok = true;
+    uint64_t solo = 0;
     if (s->cfg.plain) {
       uint64_t id = 0;
       {
@@ -621,6 +668,11 @@ void loop(sjs_server* s) {
         if (!s->pending.empty()) id = s->pending.front();
       }
       if (id) plain_one(s, id);
+    } else if ((solo = solo_candidate(s)) != 0) {
+      if (plain_one(s, solo)) {
+        std::lock_guard<std::mutex> g(s->mu);
+        ++s->stats.solo;
+      }
     } else {
       // admission (filter builds on the second stream) overlaps the steps in flight;
       // step k+1 is launched before step k's results are collected

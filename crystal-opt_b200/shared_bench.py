@@ -177,6 +177,17 @@ def serving(eng: sj.Engine, rates=(200.0, 2000.0), seconds: float = 1.0, seed: i
                            "filters_built": st.filters_built, "filters_cached": st.filters_cached})
         finally:
             srv.close()
+        # the same arrivals with lone queries sent through the plain engine
+        srv = ss.Server(eng, sc, dev, cache_filters=True, threads=threads, solo_plain=True)
+        try:
+            for t in [srv.submit(q) for q in warm]:
+                srv.wait(t, timeout_s=600.0)
+            solo, solo_rows = _poisson_run(srv, qs, rate, seed + i)
+            st = srv.stats()
+            solo.update({"steps": st.steps, "solo": st.solo, "peak_active": st.peak_active})
+        finally:
+            srv.close()
+        exact = exact and solo_rows == shared_rows
         m = min(n, plain_cap)
         srv = ss.Server(eng, sc, dev, plain=True)
         try:
@@ -184,7 +195,7 @@ def serving(eng: sj.Engine, rates=(200.0, 2000.0), seconds: float = 1.0, seed: i
         finally:
             srv.close()
         exact = exact and plain_rows == shared_rows[:m]
-        out["rates"].append({"shared": shared, "plain": plain})
+        out["rates"].append({"shared": shared, "shared_solo_plain": solo, "plain": plain})
     # saturation: every query submitted at once -- the loops' capacity
     if flood:
         qs = [ss.random_query(rng, sc) for _ in range(flood)]

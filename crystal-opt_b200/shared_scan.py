@@ -62,7 +62,7 @@ class SjbStats(C.Structure):
 class SjsConfig(C.Structure):
     _fields_ = [("limits", SjbLimits), ("step_rows", C.c_int64), ("max_active", C.c_int32),
                 ("plain", C.c_int32), ("hbm_reserve_bytes", C.c_int64), ("fault_admit_every", C.c_int32),
-                ("pad_", C.c_int32)]
+                ("solo_plain", C.c_int32)]
 
 
 class SjsTicketInfo(C.Structure):
@@ -75,7 +75,7 @@ class SjsStats(C.Structure):
                 ("rejected", C.c_uint64), ("steps", C.c_uint64), ("rows_scanned", C.c_uint64),
                 ("filters_built", C.c_uint64), ("filters_cached", C.c_uint64), ("peak_active", C.c_uint64),
                 ("busy_s", C.c_double), ("admit_s", C.c_double), ("scan_s", C.c_double),
-                ("probe_device_s", C.c_double)]
+                ("probe_device_s", C.c_double), ("solo", C.c_uint64)]
 
 
 SYMBOLS = ["sjb_batch_create", "sjb_batch_destroy", "sjb_batch_run", "sjb_batch_get_stats",
@@ -339,7 +339,7 @@ class Server:
 
     def __init__(self, eng: sj.Engine, schema: sj.StarSchema, cols: Dict[str, Any], plain=False, step_rows=0,
                  max_active=0, cache_filters=True, group_entries=0, filter_cache_bytes=0, threads=0,
-                 hbm_reserve_bytes=0, fault_admit_every=0):
+                 hbm_reserve_bytes=0, fault_admit_every=0, solo_plain=False):
         self.lib = load()
         self.eng, self.schema = eng, schema
         self._schema, self._keep = make_schema(schema, cols)
@@ -350,6 +350,7 @@ class Server:
         cfg.plain = 1 if plain else 0
         cfg.hbm_reserve_bytes = hbm_reserve_bytes
         cfg.fault_admit_every = fault_admit_every
+        cfg.solo_plain = 1 if solo_plain else 0
         h = C.c_void_p()
         sj.check(self.lib.sjs_server_create(eng.h, C.byref(self._schema), C.byref(cfg), C.byref(h)))
         self.h = h

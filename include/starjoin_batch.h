@@ -134,7 +134,10 @@ typedef struct sjs_config {
   int64_t hbm_reserve_bytes;         /* device memory left free for others (0 = 2 GiB) */
   int32_t fault_admit_every;         /* fault injection (tests): every k-th admission fails as if its
                                         device allocation had failed (SJ_ERR_OUT_OF_MEMORY); 0 = off */
-  int32_t pad_;
+  int32_t solo_plain;                /* 1: while no query is scanning and exactly one waits, that query runs
+                                        through the plain engine (low-load latency; same answer) when its row
+                                        range fits in one scan step and its group space fits the plain engine;
+                                        0 = every query joins the shared scan */
 } sjs_config;
 
 typedef struct sjs_ticket_info {
@@ -154,6 +157,7 @@ typedef struct sjs_stats {
   double admit_s;                    /* ... of which admitting (filter builds, layout) */
   double scan_s;                     /* ... of which scan steps (probe, results) */
   double probe_device_s;             /* device time of the shared-scan probes (CUDA events) */
+  uint64_t solo;                     /* queries the idle server ran through the plain engine (solo_plain) */
 } sjs_stats;
 
 sj_status sjs_server_create(sj_engine* eng, const sjb_schema* schema, const sjs_config* cfg, sjs_server** out);

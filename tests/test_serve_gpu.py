@@ -193,3 +193,58 @@ def test_destroy_releases_blocked_waiters(sj, engine, star):
     th.join(timeout=30)
     assert not th.is_alive()
     assert outcome["status"] in (0, sj.SJ_ERR_CANCELLED)
+
+
+def test_solo_plain_answers_lone_queries_exactly(oracle, engine, star):
+    """solo_plain: a query that finds the scan idle and nothing else waiting,
+    with a row range of at most one scan step, runs through the plain engine;
+    a longer lone query and a burst share the scan.  Every answer equals the
+    oracle's."""
+    sc, host, dev = star
+    rng = random.Random(16)
+    step = 1 << 19
+    lone = [ss.random_query(rng, sc, len_range=(100_000, step)) for _ in range(6)]
+    srv = ss.Server(engine, sc, dev, solo_plain=True, step_rows=step)
+    try:
+        for q in lone:  # one at a time: each finds the server idle
+            rows, info = srv.wait(srv.submit(q), timeout_s=120.0)
+            assert info.status == 0
+            assert rows == oracle.run(ss.to_plain(sc, q), host)
+        st = srv.stats()
+        assert st.solo == 6 and st.steps == 6 and st.finished == 6
+        long_q = ss.random_query(rng, sc, len_range=(4 * step, None))
+        rows, _ = srv.wait(srv.submit(long_q), timeout_s=120.0)
+        assert rows == oracle.run(ss.to_plain(sc, long_q), host)
+        st = srv.stats()
+        assert st.solo == 6 and st.steps > 7  # the shared scan, in steps
+        burst = [ss.random_query(rng, sc, len_range=(100_000, None)) for _ in range(40)]
+        tickets = [srv.submit(q) for q in burst]
+        for q, t in zip(burst, tickets):
+            rows, info = srv.wait(t, timeout_s=120.0)
+            assert rows == oracle.run(ss.to_plain(sc, q), host)
+        st = srv.stats()
+        assert st.finished == 47 and st.solo < 47 and st.peak_active > 1
+    finally:
+        srv.close()
+
+
+def test_solo_plain_cancelled_ticket(sj, engine, star):
+    """A lone query cancelled while the plain engine runs it completes as
+    cancelled, with no rows."""
+    sc, _, dev = star
+    srv = ss.Server(engine, sc, dev, solo_plain=True)
+    try:
+        q = {"preds": [{"dim": 0, "kind": "all", "group_attr": 0}, {"dim": 3, "kind": "all", "group_attr": 0}],
+             "row_range": (0, 1_000_000)}  # within one default step (fact_rows / 8, at least 2^20)
+        t = srv.submit(q)
+        srv.cancel(t)
+        try:
+            rows, info = srv.wait(t, timeout_s=60.0)
+            assert info.status == 0  # finished before the cancel reached it
+        except sj.StarJoinError as e:
+            assert e.status == sj.SJ_ERR_CANCELLED
+        ok = {"preds": [{"dim": 3, "kind": "all", "group_attr": 0}], "row_range": (0, 5000)}
+        rows, _ = srv.wait(srv.submit(ok), timeout_s=60.0)
+        assert sum(r[-2] for r in rows) == 5000
+    finally:
+        srv.close()
