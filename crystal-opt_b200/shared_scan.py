@@ -131,7 +131,47 @@ def schema_dims(schema: sj.StarSchema) -> List[Tuple[str, str, str, int, int, Li
     return dims
 
 
-def make_schema(schema: sj.StarSchema, cols: Dict[str, Any]) -> Tuple[SjbSchema, list]:
+def ssb_dims(schema: sj.StarSchema) -> List[Tuple[str, str, str, int, int, List[Tuple[str, Tuple[int, int]]]]]:
+    """The dimensions with SSB's attributes (the nested codes of the reference's
+    queries: src/ssb-jo/q2x..q4x build kernels), in the layout of schema_dims."""
+    dims = [
+        ("supp", "fk_supp", "s_key", 0, schema.supp_rows,
+         [("s_city", (0, 249)), ("s_nation", (0, 24)), ("s_region", (0, 4)), ("s_key", (1, schema.supp_rows))]),
+        ("cust", "fk_cust", "c_key", 0, schema.cust_rows,
+         [("c_city", (0, 249)), ("c_nation", (0, 24)), ("c_region", (0, 4)), ("c_key", (1, schema.cust_rows))]),
+    ]
+    if schema.part_rows:
+        dims.append(("part", "fk_part", "p_key", 0, schema.part_rows,
+                     [("p_brand1", (0, 999)), ("p_category", (0, 24)), ("p_mfgr", (0, 4)),
+                      ("p_key", (1, schema.part_rows))]))
+    dims.append(("date", "fk_date", "d_key", sj.DATE_MIN, sj.DATE_MAX - sj.DATE_MIN + 1,
+                 [("d_year", (1992, 1998)), ("d_yearmonthnum", (199201, 199812)),
+                  ("d_key", (sj.DATE_MIN, sj.DATE_MAX))]))
+    return dims
+
+
+def from_plain(q: Dict[str, Any], dims) -> Dict[str, Any]:
+    """A plain single-query description (starjoin.q21_query ... q43_query) in
+    shared-scan form over `dims`; predicates keep the plain query's dimension
+    order, so result tuples compare with oracle.run / Engine.run directly."""
+    where = {fk: i for i, (_, fk, *_rest) in enumerate(dims)}
+    preds = []
+    for d in q["dims"]:
+        i = where[d["fk"]]
+        names = [a for a, _ in dims[i][5]]
+        pred = d["pred"]
+        p: Dict[str, Any] = {"dim": i, "kind": pred[0]}
+        if pred[0] == "in":
+            p.update(attr=names.index(d["attr"]), codes=list(pred[1]))
+        elif pred[0] == "range":
+            p.update(attr=names.index(d["attr"]), lo=int(pred[1]), hi=int(pred[2]))
+        p["group_attr"] = names.index(d["payload"]) if d.get("group") else -1
+        preds.append(p)
+    return {"preds": preds, "row_range": tuple(q["row_range"])}
+
+
+def make_schema(schema: sj.StarSchema, cols: Dict[str, Any], dims=None,
+                measure_sub: Optional[str] = None) -> Tuple[SjbSchema, list]:
     s = SjbSchema()
     keep = []
 
@@ -140,7 +180,7 @@ def make_schema(schema: sj.StarSchema, cols: Dict[str, Any]) -> Tuple[SjbSchema,
         keep.append(t)
         return t.data_ptr() if hasattr(t, "data_ptr") else t.ctypes.data
 
-    dims = schema_dims(schema)
+    dims = dims or schema_dims(schema)
     s.n_dims = len(dims)
     for i, (_, fk, key, kmin, ln, attrs) in enumerate(dims):
         d = s.dims[i]
@@ -153,7 +193,7 @@ def make_schema(schema: sj.StarSchema, cols: Dict[str, Any]) -> Tuple[SjbSchema,
         for a, (name, _) in enumerate(attrs):
             d.attr[a] = ptr(name)
     s.measure = ptr("revenue")
-    s.measure_sub = None
+    s.measure_sub = ptr(measure_sub) if measure_sub else None
     s.fact_rows = schema.fact_rows
     return s, keep
 
@@ -242,10 +282,10 @@ def fill_query(q: Dict[str, Any], out: SjbQuery, keep: list) -> None:
     out.row_begin, out.row_end = q["row_range"]
 
 
-def to_plain(schema: sj.StarSchema, q: Dict[str, Any]) -> Dict[str, Any]:
+def to_plain(schema: sj.StarSchema, q: Dict[str, Any], dims=None, measure_sub: Optional[str] = None) -> Dict[str, Any]:
     """The same query as a plain single-query description (oracle / plain engine),
     with the dimensions in predicate order and a direct (exact) filter."""
-    dims = schema_dims(schema)
+    dims = dims or schema_dims(schema)
     out = []
     for p in q["preds"]:
         _, fk, key, kmin, ln, attrs = dims[p["dim"]]
@@ -260,7 +300,7 @@ def to_plain(schema: sj.StarSchema, q: Dict[str, Any]) -> Dict[str, Any]:
         out.append({"fk": fk, "key": key, "attr": attrs[p.get("attr", 0)][0] if kind != "all" else None,
                     "payload": attrs[g][0] if g >= 0 else None, "key_min": kmin, "ht_len": ln, "pred": pred,
                     "group": g >= 0, "payload_range": attrs[g][1] if g >= 0 else (0, 0)})
-    return {"dims": out, "measure": "revenue", "measure_sub": None, "row_range": tuple(q["row_range"]),
+    return {"dims": out, "measure": "revenue", "measure_sub": measure_sub, "row_range": tuple(q["row_range"]),
             "order": list(range(len(out))), "lip": True, "adaptive": False, "bf_bits_per_key": 0,
             "bf_hashes": 2}
 
@@ -282,10 +322,10 @@ class Batch:
 
     def __init__(self, eng: sj.Engine, schema: sj.StarSchema, cols: Dict[str, Any], use_graph=True,
                  cache_filters=False, threads=0, group_entries=0, result_rows=0, smem_group_entries=0,
-                 filter_cache_bytes=0):
+                 filter_cache_bytes=0, dims=None, measure_sub: Optional[str] = None):
         self.lib = load()
         self.eng, self.schema = eng, schema
-        self._schema, self._keep = make_schema(schema, cols)
+        self._schema, self._keep = make_schema(schema, cols, dims, measure_sub)
         lim = SjbLimits(group_entries, result_rows, filter_cache_bytes, 1 if use_graph else 0,
                         1 if cache_filters else 0, threads, smem_group_entries)
         h = C.c_void_p()

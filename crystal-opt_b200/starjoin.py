@@ -222,9 +222,10 @@ class StarSchema:
         """name -> (base column, divisor): SSB's nested codes.  A city's nation is
         city // 10 and its region nation // 5 (25 nations, 5 regions over 250
         cities); a brand's category is brand // 40 and its manufacturer
-        category // 5 (1000 brands, 25 categories, 5 manufacturers)."""
+        category // 5 (1000 brands, 25 categories, 5 manufacturers); a date's
+        d_yearmonthnum is datekey // 100 (19971231 -> 199712)."""
         d = {"c_nation": ("c_city", 10), "c_region": ("c_city", 50),
-             "s_nation": ("s_city", 10), "s_region": ("s_city", 50)}
+             "s_nation": ("s_city", 10), "s_region": ("s_city", 50), "d_yearmonthnum": ("d_key", 100)}
         if self.part_rows:
             d.update({"p_category": ("p_brand1", 40), "p_mfgr": ("p_brand1", 200)})
         return d
@@ -283,7 +284,8 @@ SSB_NAMES = {"fk_cust": "lo_custkey", "fk_supp": "lo_suppkey", "fk_part": "lo_pa
              "revenue": "lo_revenue", "supplycost": "lo_supplycost", "c_key": "c_custkey", "c_city": "c_city",
              "c_nation": "c_nation", "c_region": "c_region", "s_key": "s_suppkey", "s_city": "s_city",
              "s_nation": "s_nation", "s_region": "s_region", "p_key": "p_partkey", "p_brand1": "p_brand1",
-             "p_category": "p_category", "p_mfgr": "p_mfgr", "d_key": "d_datekey", "d_year": "d_year"}
+             "p_category": "p_category", "p_mfgr": "p_mfgr", "d_key": "d_datekey", "d_year": "d_year",
+             "d_yearmonthnum": "d_yearmonthnum"}
 
 
 def ssb_file_name(column: str) -> str:
@@ -342,8 +344,8 @@ def _dim(fk, key, attr, pred, payload=None, prange=(0, 0), ht_len=0, key_min=0):
             "pred": pred, "group": payload is not None, "payload_range": prange}
 
 
-def _date_dim(pred=("all",)):
-    return _dim("fk_date", "d_key", "d_year" if pred[0] != "all" else None, pred, "d_year", (1992, 1998),
+def _date_dim(pred=("all",), attr="d_year"):
+    return _dim("fk_date", "d_key", attr if pred[0] != "all" else None, pred, "d_year", (1992, 1998),
                 DATE_MAX - DATE_MIN + 1, DATE_MIN)
 
 
@@ -365,6 +367,29 @@ def q21_query(schema: StarSchema, order=(0, 1, 2), lip=True, bf_bits_per_key=0, 
     return _shape(dims, schema, order, lip, bf_bits_per_key, bf_hashes, adaptive)
 
 
+def _q2x_query(schema, region, brand_pred, order, lip, bpk, k, adaptive):
+    dims = [_dim("fk_supp", "s_key", "s_region", ("in", [region]), ht_len=schema.supp_rows),
+            _dim("fk_part", "p_key", "p_brand1", brand_pred, "p_brand1", (0, 999), schema.part_rows),
+            _date_dim()]
+    return _shape(dims, schema, order, lip, bpk, k, adaptive)
+
+
+def q22_query(schema: StarSchema, order=(0, 1, 2), lip=True, bf_bits_per_key=0, bf_hashes=2,
+              adaptive=False) -> Dict[str, Any]:
+    """SSB Q2.2 as src/ssb-jo/q22/0-lip.cu runs it: dims 0 = supplier (s_region == 2,
+    key-only), 1 = part (260 <= p_brand1 <= 267, payload p_brand1), 2 = date (every
+    day, payload d_year); group by (p_brand1, d_year); SUM(revenue).
+    Result tuples: (p_brand1, d_year, count, sum)."""
+    return _q2x_query(schema, 2, ("range", 260, 267), order, lip, bf_bits_per_key, bf_hashes, adaptive)
+
+
+def q23_query(schema: StarSchema, order=(0, 1, 2), lip=True, bf_bits_per_key=0, bf_hashes=2,
+              adaptive=False) -> Dict[str, Any]:
+    """SSB Q2.3 as src/ssb-jo/q23/0-lip.cu runs it: as Q2.2 with s_region == 3 and
+    p_brand1 == 260.  Result tuples: (p_brand1, d_year, count, sum)."""
+    return _q2x_query(schema, 3, ("in", [260]), order, lip, bf_bits_per_key, bf_hashes, adaptive)
+
+
 def q31_query(schema: StarSchema, order=(0, 1, 2), lip=True, bf_bits_per_key=0, bf_hashes=2,
               adaptive=False) -> Dict[str, Any]:
     """SSB Q3.1 as src/ssb-jo/q31/0-lip.cu runs it: dims 0 = customer (c_region == 2,
@@ -374,6 +399,30 @@ def q31_query(schema: StarSchema, order=(0, 1, 2), lip=True, bf_bits_per_key=0, 
     dims = [_dim("fk_cust", "c_key", "c_region", ("in", [2]), "c_nation", (0, 24), schema.cust_rows),
             _dim("fk_supp", "s_key", "s_region", ("in", [2]), "s_nation", (0, 24), schema.supp_rows),
             _date_dim(("range", 1992, 1997))]
+    return _shape(dims, schema, order, lip, bf_bits_per_key, bf_hashes, adaptive)
+
+
+def q32_query(schema: StarSchema, order=(0, 1, 2), lip=True, bf_bits_per_key=0, bf_hashes=2,
+              adaptive=False) -> Dict[str, Any]:
+    """SSB Q3.2 as src/ssb-jo/q32/0-lip.cu runs it: dims 0 = supplier (s_nation == 24,
+    payload s_city), 1 = customer (c_nation == 24, payload c_city), 2 = date
+    (1992 <= d_year <= 1997); group by (s_city, c_city, d_year); SUM(revenue) (the
+    driver sums in int32).  Result tuples: (s_city, c_city, d_year, count, sum)."""
+    dims = [_dim("fk_supp", "s_key", "s_nation", ("in", [24]), "s_city", (0, 249), schema.supp_rows),
+            _dim("fk_cust", "c_key", "c_nation", ("in", [24]), "c_city", (0, 249), schema.cust_rows),
+            _date_dim(("range", 1992, 1997))]
+    return _shape(dims, schema, order, lip, bf_bits_per_key, bf_hashes, adaptive)
+
+
+def q34_query(schema: StarSchema, order=(0, 1, 2), lip=True, bf_bits_per_key=0, bf_hashes=2,
+              adaptive=False) -> Dict[str, Any]:
+    """SSB Q3.4 as src/ssb-jo/q34/0-lip.cu runs it: dims 0 = supplier (s_city IN
+    {231, 235}), 1 = customer (c_city IN {231, 235}), 2 = date (d_yearmonthnum ==
+    199712, payload d_year); group by (s_city, c_city, d_year); SUM(revenue) (int32
+    in the driver).  Result tuples: (s_city, c_city, d_year, count, sum)."""
+    dims = [_dim("fk_supp", "s_key", "s_city", ("in", [231, 235]), "s_city", (0, 249), schema.supp_rows),
+            _dim("fk_cust", "c_key", "c_city", ("in", [231, 235]), "c_city", (0, 249), schema.cust_rows),
+            _date_dim(("range", 199712, 199712), attr="d_yearmonthnum")]
     return _shape(dims, schema, order, lip, bf_bits_per_key, bf_hashes, adaptive)
 
 
@@ -387,6 +436,36 @@ def q41_query(schema: StarSchema, order=(0, 1, 2, 3), lip=True, bf_bits_per_key=
             _dim("fk_cust", "c_key", "c_region", ("in", [1]), "c_nation", (0, 24), schema.cust_rows),
             _dim("fk_part", "p_key", "p_mfgr", ("in", [0, 1]), ht_len=schema.part_rows),
             _date_dim()]
+    return _shape(dims, schema, order, lip, bf_bits_per_key, bf_hashes, adaptive, sub="supplycost")
+
+
+def q42_query(schema: StarSchema, order=(0, 1, 2, 3), lip=False, bf_bits_per_key=0, bf_hashes=2,
+              adaptive=False) -> Dict[str, Any]:
+    """SSB Q4.2 as src/ssb-jo/q42/0-naive.cu runs it (the reference has no LIP
+    driver for it): dims 0 = supplier (s_region == 1, payload s_nation), 1 =
+    customer (c_region == 1, key-only), 2 = part (p_mfgr IN {0, 1}, payload
+    p_category), 3 = date (d_year IN {1997, 1998}, payload d_year); group by
+    (s_nation, p_category, d_year); SUM(revenue - supplycost) in uint64.
+    Result tuples: (s_nation, p_category, d_year, count, sum)."""
+    dims = [_dim("fk_supp", "s_key", "s_region", ("in", [1]), "s_nation", (0, 24), schema.supp_rows),
+            _dim("fk_cust", "c_key", "c_region", ("in", [1]), ht_len=schema.cust_rows),
+            _dim("fk_part", "p_key", "p_mfgr", ("in", [0, 1]), "p_category", (0, 24), schema.part_rows),
+            _date_dim(("range", 1997, 1998))]
+    return _shape(dims, schema, order, lip, bf_bits_per_key, bf_hashes, adaptive, sub="supplycost")
+
+
+def q43_query(schema: StarSchema, order=(0, 1, 2, 3), lip=False, bf_bits_per_key=0, bf_hashes=2,
+              adaptive=False) -> Dict[str, Any]:
+    """SSB Q4.3 as src/ssb-jo/q43/q43.cu runs it (no Bloom filters): dims 0 =
+    supplier (s_nation == 24, payload s_city), 1 = customer (c_region == 1,
+    key-only), 2 = part (p_category == 3, payload p_brand1), 3 = date (d_year IN
+    {1997, 1998}, payload d_year); group by (s_city, p_brand1, d_year);
+    SUM(revenue - supplycost) (int32 in the driver).
+    Result tuples: (s_city, p_brand1, d_year, count, sum)."""
+    dims = [_dim("fk_supp", "s_key", "s_nation", ("in", [24]), "s_city", (0, 249), schema.supp_rows),
+            _dim("fk_cust", "c_key", "c_region", ("in", [1]), ht_len=schema.cust_rows),
+            _dim("fk_part", "p_key", "p_category", ("in", [3]), "p_brand1", (0, 999), schema.part_rows),
+            _date_dim(("range", 1997, 1998))]
     return _shape(dims, schema, order, lip, bf_bits_per_key, bf_hashes, adaptive, sub="supplycost")
 
 

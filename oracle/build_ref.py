@@ -3,8 +3,8 @@
 The driver sources are compiled where they lie under the reference tree
 (default /root/reference, override with CRYSTAL_OPT_REF); nothing is copied.
 Each binary is one driver -- src/ssb-jo/q33/<order>-<lip|naive>.cu wrapped by
-ref_runner.cu, or src/ssb-jo/q{21,31,41}/0-lip.cu wrapped by ref_runner_shapes.cu --
-the wrapper supplying main() and the synthetic columns.  The reference's
+ref_runner.cu, or one of SHAPE_SOURCES (the other queries' drivers) wrapped by
+ref_runner_shapes.cu -- the wrapper supplying main() and the synthetic columns.  The reference's
 CUB 1.6.4 test header is replaced by ref_shim/cub/test/test_util.h.  Flags follow
 the reference Makefile (-O3 -lineinfo -Xptxas -dlcm=ca, Makefile:23,35) with the
 architecture switched to sm_100a.
@@ -48,15 +48,20 @@ def _compile(order: int, method: str) -> str:
     return out
 
 
-SHAPES = (21, 31, 41)  # src/ssb-jo/q21, q31, q41: order-0 LIP drivers
+# The other queries' drivers under src/ssb-jo/: the order-0 LIP driver where the
+# reference has one; Q4.2 has only a naive driver and Q4.3 a single q43.cu.
+SHAPE_SOURCES = {21: "q21/0-lip.cu", 22: "q22/0-lip.cu", 23: "q23/0-lip.cu", 31: "q31/0-lip.cu",
+                 32: "q32/0-lip.cu", 34: "q34/0-lip.cu", 41: "q41/0-lip.cu", 42: "q42/0-naive.cu",
+                 43: "q43/q43.cu"}
+SHAPES = tuple(SHAPE_SOURCES)
 
 
 def shape_binary(query: int) -> str:
-    return os.path.join(OUT, f"q{query}_0_lip")
+    return os.path.join(OUT, f"q{query}_ref")
 
 
 def _compile_shape(query: int) -> str:
-    src = os.path.join(REF, "src", "ssb-jo", f"q{query}", "0-lip.cu")
+    src = os.path.join(REF, "src", "ssb-jo", SHAPE_SOURCES[query])
     out = shape_binary(query)
     runner = os.path.join(HERE, "ref_runner_shapes.cu")
     deps = [src, runner, os.path.join(HERE, "ref_shim", "cub", "test", "test_util.h")]
@@ -64,6 +69,8 @@ def _compile_shape(query: int) -> str:
         return out
     cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
            "-Xptxas", "-dlcm=ca", "-I", REF, "-I", os.path.join(HERE, "ref_shim"),
+           # q42/0-naive.cu and q43/q43.cu name gpu_utils.h / ssb_utils.h without their src/ssb/ directory
+           "-I", os.path.join(REF, "src", "ssb"),
            f'-DREF_DRIVER="{src}"', f"-DREF_QUERY={query}", "-o", out + ".tmp", runner]
     subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
     os.replace(out + ".tmp", out)
@@ -71,8 +78,8 @@ def _compile_shape(query: int) -> str:
 
 
 def build(jobs: int = 0) -> list[str]:
-    """Build the 12 Q3.3 drivers and the Q2.1 / Q3.1 / Q4.1 LIP drivers
-    (skipped when the reference tree is absent)."""
+    """Build the 12 Q3.3 drivers and the other queries' drivers (SHAPE_SOURCES);
+    skipped when the reference tree is absent."""
     if not available():
         return []
     os.makedirs(OUT, exist_ok=True)

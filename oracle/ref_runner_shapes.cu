@@ -1,10 +1,11 @@
 // ref_runner_shapes.cu -- TEST INFRASTRUCTURE: a main() around one of the
-// reference's own SSB Q2.1 / Q3.1 / Q4.1 LIP drivers (src/ssb-jo/q{21,31,41}/0-lip.cu),
-// compiled unmodified from its source tree by build_ref.py into oracle/_ref/.
-// It feeds the driver the seeded synthetic columns the engine's tests use (SSB's
-// nested codes derived as nation = city / 10, region = city / 50,
-// category = brand / 40, mfgr = brand / 200) and calls the driver's own
-// runQuery(), which prints one line per group.  REF_QUERY selects the driver.
+// reference's own SSB drivers other than Q3.3: src/ssb-jo/q{21,22,23,31,32,34,41}/0-lip.cu,
+// src/ssb-jo/q42/0-naive.cu and src/ssb-jo/q43/q43.cu, compiled unmodified from
+// its source tree by build_ref.py into oracle/_ref/.  It feeds the driver the
+// seeded synthetic columns the engine's tests use (SSB's nested codes derived as
+// nation = city / 10, region = city / 50, category = brand / 40,
+// mfgr = brand / 200, d_yearmonthnum = datekey / 100) and calls the driver's
+// own runQuery(), which prints one line per group.  REF_QUERY selects the driver.
 #define main crystal_reference_driver_main
 #include REF_DRIVER
 #undef main
@@ -66,6 +67,7 @@ int main(int argc, char** argv) {
   auto h_s_nation = div_by(h_s_city, 10), h_s_region = div_by(h_s_city, 50);
   auto h_c_nation = div_by(h_c_city, 10), h_c_region = div_by(h_c_city, 50);
   auto h_p_category = div_by(h_p_brand1, 40), h_p_mfgr = div_by(h_p_brand1, 200);
+  auto h_d_yearmonthnum = div_by(h_d_datekey, 100);
 
   int* lo_orderdate = to_gpu(h_lo_orderdate, n);
   int* lo_suppkey = to_gpu(h_lo_suppkey, n);
@@ -84,6 +86,35 @@ int main(int argc, char** argv) {
   fflush(stdout);
   runQuery(lo_orderdate, lo_partkey, lo_suppkey, lo_revenue, n, p_partkey, p_brand1, p_category, p_len, d_datekey,
            d_year, d_len, s_suppkey, s_region, s_len, g_allocator);
+#elif REF_QUERY == 22 || REF_QUERY == 23
+  int* lo_partkey = to_gpu(h_lo_partkey, n);
+  int* p_partkey = to_gpu(h_p_partkey, p_len);
+  int* p_brand1 = to_gpu(h_p_brand1, p_len);
+  CubDebugExit(cudaDeviceSynchronize());
+  fflush(stdout);
+  runQuery(lo_orderdate, lo_partkey, lo_suppkey, lo_revenue, n, p_partkey, p_brand1, p_len, d_datekey, d_year, d_len,
+           s_suppkey, s_region, s_len, g_allocator);
+#elif REF_QUERY == 32
+  int* lo_custkey = to_gpu(h_lo_custkey, n);
+  int* s_nation = to_gpu(h_s_nation, s_len);
+  int* s_city = to_gpu(h_s_city, s_len);
+  int* c_custkey = to_gpu(h_c_custkey, c_len);
+  int* c_nation = to_gpu(h_c_nation, c_len);
+  int* c_city = to_gpu(h_c_city, c_len);
+  CubDebugExit(cudaDeviceSynchronize());
+  fflush(stdout);
+  runQuery(lo_orderdate, lo_custkey, lo_suppkey, lo_revenue, n, d_datekey, d_year, d_len, s_suppkey, s_nation,
+           s_city, s_len, c_custkey, c_nation, c_city, c_len, g_allocator);
+#elif REF_QUERY == 34
+  int* lo_custkey = to_gpu(h_lo_custkey, n);
+  int* d_yearmonthnum = to_gpu(h_d_yearmonthnum, d_len);
+  int* s_city = to_gpu(h_s_city, s_len);
+  int* c_custkey = to_gpu(h_c_custkey, c_len);
+  int* c_city = to_gpu(h_c_city, c_len);
+  CubDebugExit(cudaDeviceSynchronize());
+  fflush(stdout);
+  runQuery(lo_orderdate, lo_custkey, lo_suppkey, lo_revenue, n, d_datekey, d_year, d_yearmonthnum, d_len,
+           s_suppkey, s_city, s_len, c_custkey, c_city, c_len, g_allocator);
 #elif REF_QUERY == 31
   int* lo_custkey = to_gpu(h_lo_custkey, n);
   int* s_nation = to_gpu(h_s_nation, s_len);
@@ -107,8 +138,39 @@ int main(int argc, char** argv) {
   fflush(stdout);
   runQuery(lo_orderdate, lo_custkey, lo_partkey, lo_suppkey, lo_revenue, lo_supplycost, n, d_datekey, d_year, d_len,
            p_partkey, p_mfgr, p_len, s_suppkey, s_region, s_len, c_custkey, c_region, c_nation, c_len, g_allocator);
+#elif REF_QUERY == 42
+  int* lo_custkey = to_gpu(h_lo_custkey, n);
+  int* lo_partkey = to_gpu(h_lo_partkey, n);
+  int* lo_supplycost = to_gpu(h_lo_supplycost, n);
+  int* p_partkey = to_gpu(h_p_partkey, p_len);
+  int* p_mfgr = to_gpu(h_p_mfgr, p_len);
+  int* p_category = to_gpu(h_p_category, p_len);
+  int* s_nation = to_gpu(h_s_nation, s_len);
+  int* c_custkey = to_gpu(h_c_custkey, c_len);
+  int* c_region = to_gpu(h_c_region, c_len);
+  CubDebugExit(cudaDeviceSynchronize());
+  fflush(stdout);
+  runQuery(lo_orderdate, lo_custkey, lo_partkey, lo_suppkey, lo_revenue, lo_supplycost, n, d_datekey, d_year, d_len,
+           p_partkey, p_mfgr, p_category, p_len, s_suppkey, s_region, s_nation, s_len, c_custkey, c_region, c_len,
+           g_allocator);
+#elif REF_QUERY == 43
+  int* lo_custkey = to_gpu(h_lo_custkey, n);
+  int* lo_partkey = to_gpu(h_lo_partkey, n);
+  int* lo_supplycost = to_gpu(h_lo_supplycost, n);
+  int* p_partkey = to_gpu(h_p_partkey, p_len);
+  int* p_category = to_gpu(h_p_category, p_len);
+  int* p_brand1 = to_gpu(h_p_brand1, p_len);
+  int* s_nation = to_gpu(h_s_nation, s_len);
+  int* s_city = to_gpu(h_s_city, s_len);
+  int* c_custkey = to_gpu(h_c_custkey, c_len);
+  int* c_region = to_gpu(h_c_region, c_len);
+  CubDebugExit(cudaDeviceSynchronize());
+  fflush(stdout);
+  runQuery(lo_orderdate, lo_custkey, lo_partkey, lo_suppkey, lo_revenue, lo_supplycost, n, d_datekey, d_year, d_len,
+           p_partkey, p_category, p_brand1, p_len, s_suppkey, s_nation, s_city, s_len, c_custkey, c_region, c_len,
+           g_allocator);
 #else
-#error "REF_QUERY must be 21, 31 or 41"
+#error "REF_QUERY must be 21, 22, 23, 31, 32, 34, 41, 42 or 43"
 #endif
   fflush(stdout);
   return 0;

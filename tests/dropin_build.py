@@ -1,6 +1,6 @@
-"""Build the reference's own SSB drivers (the 12 Q3.3 drivers and the Q2.1 /
-Q3.1 / Q4.1 LIP drivers) against this repository's crystal/*.cuh device
-functions (the drop-in check).
+"""Build the reference's own SSB drivers (the 12 Q3.3 drivers and the drivers of
+Q2.1-Q2.3, Q3.1, Q3.2, Q3.4 and Q4.1-Q4.3) against this repository's
+crystal/*.cuh device functions (the drop-in check).
 
 Each driver (src/ssb-jo/q33/<order>-<lip|naive>.cu, compiled where it lies in
 the reference tree, default /root/reference or $CRYSTAL_OPT_REF) includes
@@ -50,16 +50,19 @@ def _compile(order: int, method: str) -> str:
     return out
 
 
-SHAPES = (21, 31, 41)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+from build_ref import SHAPE_SOURCES  # noqa: E402  (driver file of each other query)
+
+SHAPES = tuple(SHAPE_SOURCES)
 
 
 def shape_binary(query: int) -> str:
-    return os.path.join(OUT, f"q{query}_0_lip")
+    return os.path.join(OUT, f"q{query}_ref")
 
 
 def _compile_shape(query: int) -> str:
-    """src/ssb-jo/q<query>/0-lip.cu against crystal/*.cuh, main() from oracle/ref_runner_shapes.cu."""
-    src = os.path.join(REF, "src", "ssb-jo", f"q{query}", "0-lip.cu")
+    """The query's reference driver against crystal/*.cuh, main() from oracle/ref_runner_shapes.cu."""
+    src = os.path.join(REF, "src", "ssb-jo", SHAPE_SOURCES[query])
     out = shape_binary(query)
     runner = os.path.join(ROOT, "oracle", "ref_runner_shapes.cu")
     hdrs = [os.path.join(ROOT, "crystal-opt_b200", "crystal", f) for f in os.listdir(
@@ -69,6 +72,7 @@ def _compile_shape(query: int) -> str:
         return out
     cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
            "-I", os.path.join(ROOT, "crystal-opt_b200"), "-I", os.path.join(ROOT, "oracle", "ref_shim"),
+           "-I", os.path.join(REF, "src", "ssb"),  # gpu_utils.h / ssb_utils.h named without src/ssb/
            f'-DREF_DRIVER="{src}"', f"-DREF_QUERY={query}", "-o", out + ".tmp", runner]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

@@ -6,7 +6,7 @@ star schema and records the groups each prints: (d_year, c_city, s_city, int32
 SUM(lo_revenue)).  Needs a GPU; run from the repository root:
 
     python tests/golden/make_golden.py            # Q3.3, all 12 drivers
-    python tests/golden/make_golden.py --shapes   # Q2.1 / Q3.1 / Q4.1
+    python tests/golden/make_golden.py --shapes   # Q2.1-Q2.3, Q3.1, Q3.2, Q3.4, Q4.1-Q4.3
 """
 import json
 import os
@@ -31,16 +31,24 @@ def run_driver(order: int, method: str, schema, trials: int = 1, probe_trials: i
 
 
 def shapes():
-    """Groups printed by the reference's Q2.1 / Q3.1 / Q4.1 LIP drivers
-    (oracle/_ref/q{21,31,41}_0_lip) on the seeded SF1-sized schema."""
+    """Groups printed by the reference's drivers for the other queries
+    (oracle/_ref/q<query>_ref, built from build_ref.SHAPE_SOURCES) on the seeded
+    SF1-sized schema."""
     from workloads import SHAPES_SMALL, SHAPE_WIDTH
     sc = SHAPES_SMALL
-    rec = {"what": "groups printed by the reference's src/ssb-jo/q{21,31,41}/0-lip.cu drivers on the seeded "
-                   "schema; columns as each driver prints them",
+    rec = {"what": "groups printed by the reference's src/ssb-jo drivers " +
+                   ", ".join(build_ref.SHAPE_SOURCES.values()) + " on the seeded schema; columns as each "
+                   "driver prints them",
            "schema": {"seed": sc.seed, "fact_rows": sc.fact_rows, "cust_rows": sc.cust_rows,
                       "supp_rows": sc.supp_rows, "part_rows": sc.part_rows},
-           "columns": {"21": ["d_year", "p_brand1", "sum_u64"], "31": ["d_year", "c_nation", "s_nation", "sum_u64"],
-                       "41": ["d_year", "c_nation", "sum_u64(revenue-supplycost)"]},
+           "columns": {"21": ["d_year", "p_brand1", "sum_u64"], "22": ["d_year", "p_brand1", "sum_u64"],
+                       "23": ["d_year", "p_brand1", "sum_u64"],
+                       "31": ["d_year", "c_nation", "s_nation", "sum_u64"],
+                       "32": ["d_year", "c_city", "s_city", "sum_int32"],
+                       "34": ["d_year", "c_city", "s_city", "sum_int32"],
+                       "41": ["d_year", "c_nation", "sum_u64(revenue-supplycost)"],
+                       "42": ["d_year", "s_nation", "p_category", "sum_u64(revenue-supplycost)"],
+                       "43": ["d_year", "s_city", "p_brand1", "sum_int32(revenue-supplycost)"]},
            "groups": {}}
     for q in build_ref.SHAPES:
         cmd = [build_ref.shape_binary(q), f"--seed={sc.seed}", f"--n={sc.fact_rows}", f"--c={sc.cust_rows}",

@@ -36,9 +36,9 @@ def test_reference_driver_on_b200_device_api(sj, oracle, torch_cuda, order, meth
         assert got == sorted(tuple(r) for r in json.load(f)["groups"])
 
 
-@pytest.mark.parametrize("query", [21, 31, 41])
+@pytest.mark.parametrize("query", sorted(dropin_build.SHAPES))
 def test_reference_shape_driver_on_b200_device_api(sj, oracle, torch_cuda, query):
-    """The reference's own Q2.1 / Q3.1 / Q4.1 LIP drivers, compiled unmodified
+    """The reference's own drivers of the other queries, compiled unmodified
     against crystal/*.cuh, print the oracle's groups and the golden vectors of
     the same drivers built against the reference's headers."""
     from workloads import SHAPE_QUERIES, SHAPE_WIDTH, SHAPES_SMALL, shape_as_printed

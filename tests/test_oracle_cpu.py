@@ -127,9 +127,10 @@ def test_oracle_matches_reference_cuda_golden(sj, oracle):
 
 def test_oracle_matches_reference_shape_golden(sj, oracle):
     """Pins the oracle on the other query shapes: groups printed by the
-    reference's own Q2.1 / Q3.1 / Q4.1 LIP drivers (oracle/_ref, run on a B200)
-    on the seeded SF1-sized schema; their sums are uint64 (Q4.1: revenue -
-    supplycost, two's complement)."""
+    reference's own drivers of Q2.1-Q2.3, Q3.1, Q3.2, Q3.4 and Q4.1-Q4.3
+    (oracle/_ref, run on a B200) on the seeded SF1-sized schema.  Q2.x, Q3.1,
+    Q4.1 and Q4.2 sum in uint64 (Q4.x: revenue - supplycost, two's complement);
+    Q3.2, Q3.4 and Q4.3 print an int32 sum."""
     from workloads import SHAPE_QUERIES, shape_as_printed
     g = _golden("shapes_small_reference.json")
     sc = sj.StarSchema(**g["schema"])

@@ -88,3 +88,20 @@ def test_plain_restatement_runs_through_the_oracle(oracle):
             groups[k] = (c + 1, (s + int(rev[i])) % (1 << 64))
         want = sorted(k + v for k, v in groups.items())
         assert got == want
+
+
+def test_ssb_shapes_round_trip_through_shared_form(sj, oracle):
+    """Every SSB query shape (Q2.1-Q4.3 as the reference's drivers run them)
+    restated in shared-scan form over the SSB-attribute dimensions and back
+    answers like the original on the oracle."""
+    from workloads import SHAPE_QUERIES
+    sc = sj.StarSchema(seed=0x5EED0011, fact_rows=200_000, cust_rows=3_000, supp_rows=200, part_rows=20_000)
+    cols = sj.gen_host(sc)
+    dims = ss.ssb_dims(sc)
+    for q, make in SHAPE_QUERIES.items():
+        plain = make(sc)
+        shared = ss.from_plain(plain, dims)
+        assert [p["dim"] for p in shared["preds"]] == [
+            [d[1] for d in dims].index(x["fk"]) for x in plain["dims"]], q
+        back = ss.to_plain(sc, shared, dims, plain["measure_sub"])
+        assert oracle.run(back, cols) == oracle.run(plain, cols), q

@@ -22,22 +22,40 @@ REF_DRIVER_ORDERS = {
 
 SMALL = sj.StarSchema(seed=0x5EED0001, fact_rows=6_000_000, cust_rows=30_000, supp_rows=2_000)
 FULL = sj.StarSchema(seed=0x5EED0002, fact_rows=120_000_000, cust_rows=600_000, supp_rows=40_000)
-# SSB scale-factor-1 dimension sizes for the Q2.1 / Q3.1 / Q4.1 shapes
+# SSB scale-factor-1 dimension sizes for the Q2.x / Q3.1 / Q3.2 / Q3.4 / Q4.x shapes
 SHAPES_SMALL = sj.StarSchema(seed=0x5EED0009, fact_rows=6_000_000, cust_rows=30_000, supp_rows=2_000,
                              part_rows=200_000)
-SHAPE_QUERIES = {21: sj.q21_query, 31: sj.q31_query, 41: sj.q41_query}
-SHAPE_WIDTH = {21: 3, 31: 4, 41: 3}  # integers per group line the reference drivers print
+SHAPE_QUERIES = {21: sj.q21_query, 22: sj.q22_query, 23: sj.q23_query, 31: sj.q31_query, 32: sj.q32_query,
+                 34: sj.q34_query, 41: sj.q41_query, 42: sj.q42_query, 43: sj.q43_query}
+# integers per group line the reference drivers print
+SHAPE_WIDTH = {21: 3, 22: 3, 23: 3, 31: 4, 32: 4, 34: 4, 41: 3, 42: 4, 43: 4}
+
+
+def _int32(v: int) -> int:
+    return ((v + 2 ** 31) % 2 ** 32) - 2 ** 31
 
 
 def shape_as_printed(query: int, rows: List[tuple]) -> List[tuple]:
     """Engine / oracle result tuples in the order the reference drivers print
-    them: Q2.1 (d_year, p_brand1, sum), Q3.1 (d_year, c_nation, s_nation, sum),
-    Q4.1 (d_year, c_nation, sum) -- src/ssb-jo/q{21,31,41}/0-lip.cu result loops."""
-    if query == 21:
+    them (the result loops of src/ssb-jo/q*/ drivers):
+    Q2.x (d_year, p_brand1, uint64 sum); Q3.1 (d_year, c_nation, s_nation, uint64
+    sum); Q3.2 / Q3.4 (d_year, c_city, s_city, int32 sum); Q4.1 (d_year, c_nation,
+    uint64 sum); Q4.2 (d_year, s_nation, p_category, uint64 sum); Q4.3 (d_year,
+    s_city, p_brand1, int32 sum).  Drivers that accumulate in int32 print the
+    low 32 bits of the sum as a signed value."""
+    if query in (21, 22, 23):
         return sorted((y, b, v) for (b, y, c, v) in rows)
     if query == 31:
         return sorted((y, cn, sn, v) for (cn, sn, y, c, v) in rows)
-    return sorted((y, cn, v) for (cn, y, c, v) in rows)
+    if query in (32, 34):
+        return sorted((y, cc, sc, _int32(v)) for (sc, cc, y, c, v) in rows)
+    if query == 41:
+        return sorted((y, cn, v) for (cn, y, c, v) in rows)
+    if query == 42:
+        return sorted((y, sn, cat, v) for (sn, cat, y, c, v) in rows)
+    if query == 43:
+        return sorted((y, sc, b, _int32(v)) for (sc, b, y, c, v) in rows)
+    raise ValueError(f"no shape {query}")
 
 
 FOURDIM = sj.StarSchema(seed=0x5EED0003, fact_rows=120_000_000, cust_rows=600_000, supp_rows=40_000,
