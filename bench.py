@@ -430,10 +430,15 @@ def main():
     ap.add_argument("--sweep4", type=int, nargs="?", const=256, default=None,
                     help="run only the 4-dimension selectivity x filter sweep (optionally the first N of its "
                          "256 selectivity settings)")
+    ap.add_argument("--shapes", action="store_true",
+                    help="run only the SSB query shapes (Q2.1-Q4.3) at 120M rows: this engine, or with "
+                         "--impl reference the reference's own CUDA drivers on the same schema")
     args = ap.parse_args()
     FACT_ROWS = args.rows
     args.warmup = max(3, args.warmup)
-    if args.sweep4 is not None:
+    if args.shapes:
+        run_shapes(args)
+    elif args.sweep4 is not None:
         import itertools
         import starjoin as sj
         import sweep_bench
@@ -447,6 +452,47 @@ def main():
         run_reference(args)
     else:
         run_engine(args)
+
+
+def run_shapes(args):
+    """Every SSB query shape at 120M rows: this engine (shapes_bench), or the
+    reference's own unmodified CUDA drivers (oracle/_ref) on the same seeded
+    schema with their `time_query`; groups_sha1 digests compare the two."""
+    import shapes_bench
+    if args.impl != "reference":
+        import starjoin as sj
+        eng = sj.Engine(0)
+        print(json.dumps({"shapes": shapes_bench.shapes(eng, reps=max(3, min(args.steps, 20)))}), flush=True)
+        eng.close()
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import build_ref
+    sc = shapes_bench.SCHEMA
+    width = {21: 3, 22: 3, 23: 3, 31: 4, 32: 4, 33: 4, 34: 4, 41: 3, 42: 4, 43: 4}
+    trials = max(3, min(args.steps, 10))
+    out = {"impl": "reference", "workload": "SSB query shapes, reference CUDA drivers (unmodified, sm_100a)",
+           "queries": {}}
+    for q in shapes_bench.QUERIES:
+        exe = build_ref.binary(0, "lip") if q == 33 else build_ref.shape_binary(q)
+        if not os.path.exists(exe):
+            out["queries"][str(q)] = {"unavailable": "oracle/_ref not built"}
+            continue
+        cmd = [exe, f"--seed={sc['seed']}", f"--n={sc['fact_rows']}", f"--c={sc['cust_rows']}",
+               f"--s={sc['supp_rows']}", f"--t={trials}"]
+        if q != 33:
+            cmd.append(f"--p={sc['part_rows']}")
+        try:
+            text = subprocess.run(cmd, capture_output=True, text=True, timeout=600, check=True).stdout
+        except Exception as e:  # noqa: BLE001
+            out["queries"][str(q)] = {"unavailable": f"driver failed: {type(e).__name__}"}
+            continue
+        tq = build_ref.parse_output(text)["time_query_ms"]
+        tq = tq[1:] or tq  # the first call also pays the caching allocator's first allocations
+        groups = build_ref.parse_groups(text, width[q])
+        out["queries"][str(q)] = {"driver": build_ref.SHAPE_SOURCES.get(q, "q33/0-lip.cu"),
+                                  "time_query_ms": statistics.median(tq), "groups": len(groups),
+                                  "groups_sha1": shapes_bench.groups_digest(groups)}
+    print(json.dumps({"shapes": out}), flush=True)
 
 
 def run_shared(args):

@@ -3,7 +3,8 @@
 // Candidates are timed on the plan's own device columns with CUDA events around
 // sj_query_probe (the build is re-run before every timed probe, as a query
 // would).  Search order, each step keeping the best so far:
-//   1. filter kind   direct bitmap, or 4 / 8 / 16 bits per key x 1..4 bits set
+//   1. filter kind   direct bitmap, per-dimension auto layout (x 2..3 bits set),
+//                    or 4 / 8 / 16 bits per key x 1..4 bits set
 //   2. geometry      threads x rows per lane, then rows per stage x stages
 //   3. join order    most selective first, or every permutation
 // The groups of every candidate are compared with the first candidate's.
@@ -209,9 +210,10 @@ extern "C" sj_status sj_autotune(sj_engine* eng, sj_plan* plan, const sj_autotun
   // 1. filter kind
   if (o.tune_filter) {
     const sj_plan start = best;
-    const int bpks[] = {0, 4, 8, 16};
+    const int bpks[] = {0, SJ_BF_AUTO, 4, 8, 16};
     for (int bpk : bpks)
-      for (int k = 1; k <= (bpk ? 4 : 1); ++k) {
+      for (int k = 1; k <= (bpk > 0 ? 4 : (bpk < 0 ? 3 : 1)); ++k) {
+        if (bpk < 0 && k == 1) continue;  // auto: 2 or 3 bits per key where it goes blocked
         sj_plan c = start;
         c.bf_bits_per_key = bpk;
         c.bf_hashes = bpk ? k : 2;

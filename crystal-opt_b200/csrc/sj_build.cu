@@ -96,9 +96,9 @@ __device__ void choose_start(const SjPlanRt& P, SjDesc* desc) {
   for (uint32_t d = 0; d < n; ++d) {
     const SjDimRt& D = P.dim[d];
     const uint32_t ins = desc->dim[d].n_inserted;
-    const uint32_t l2 = (D.bf_mode == kBfBlocked) ? bf_blocked_log2(ins, D.bf_bits_per_key, D.bf_max_log2)
-                                                  : D.bf_max_log2;
-    bytes[d] = (D.bf_mode == kBfDirect) ? max(8u, (1u << l2) / 8u) : (8u << l2);
+    uint32_t l2;
+    const uint32_t mode = bf_effective(D.bf_mode, D.bf_max_log2, D.bf_bits_per_key, ins, P.bf_smem_budget, &l2);
+    bytes[d] = (mode == kBfDirect) ? max(8u, (1u << l2) / 8u) : (8u << l2);
     rate[d] = ((float)ins + 1.f) / ((float)D.rows + 2.f);
   }
   auto place = [&](const uint32_t* ord, uint32_t* off, float* weight) {
@@ -162,13 +162,16 @@ __global__ void __launch_bounds__(256) sj_dim_insert(const __grid_constant__ SjP
   SjDesc* desc = P.desc;
 
   const uint32_t n_ins = desc->dim[d].n_inserted;
-  const uint32_t log2 = (D.bf_mode == kBfBlocked) ? bf_blocked_log2(n_ins, D.bf_bits_per_key, D.bf_max_log2)
-                                                  : D.bf_max_log2;
+  uint32_t log2;
+  const uint32_t mode = bf_effective(D.bf_mode, D.bf_max_log2, D.bf_bits_per_key, n_ins, P.bf_smem_budget, &log2);
   const uint32_t pwords = D.grouped ? (D.payload_span + 31u) / 32u : 0u;
   if (D.grouped) bitmap_prefix(D.payload_bitmap, pwords, prefix, &s_total);
 
   if (blockIdx.x == 0) {
-    if (threadIdx.x == 0) desc->dim[d].bf_log2 = log2;
+    if (threadIdx.x == 0) {
+      desc->dim[d].bf_log2 = log2;
+      desc->dim[d].bf_mode = mode;
+    }
     if (D.grouped) {
       // dictionary: code -> payload value
       for (uint32_t w = threadIdx.x; w < pwords; w += blockDim.x) {
@@ -222,7 +225,7 @@ __global__ void __launch_bounds__(256) sj_dim_insert(const __grid_constant__ SjP
     D.ht[s].y = val;
     // Filter insert keyed by the PHT slot, so the filter never rejects a row the
     // PHT would accept.
-    if (D.bf_mode == kBfDirect) {
+    if (mode == kBfDirect) {
       uint32_t* w = reinterpret_cast<uint32_t*>(D.bf) + (s >> 5);
       uint32_t bit = 1u << (s & 31u);
       if (!(*w & bit)) atomicOr(w, bit);

@@ -174,9 +174,9 @@ static sj_status validate_plan(const sj_plan* p) {
     if (d < 0 || d >= p->n_dims || used[d]) return fail(SJ_ERR_INVALID_ARGUMENT, "order is not a permutation");
     used[d] = 1;
   }
-  if (p->bf_bits_per_key < 0 || p->bf_bits_per_key > 64)
+  if (p->bf_bits_per_key < SJ_BF_AUTO || p->bf_bits_per_key > 64)
     return fail(SJ_ERR_INVALID_ARGUMENT, "bf_bits_per_key=%d", p->bf_bits_per_key);
-  if (p->bf_bits_per_key > 0 && (p->bf_hashes < 1 || p->bf_hashes > 4))
+  if (p->bf_bits_per_key != 0 && (p->bf_hashes < 1 || p->bf_hashes > 4))
     return fail(SJ_ERR_INVALID_ARGUMENT, "bf_hashes=%d (1..4)", p->bf_hashes);
   uint64_t groups = 1;
   for (int d = 0; d < p->n_dims; ++d) {
@@ -278,7 +278,8 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
   q->plan = *plan;
   sj_plan& p = q->plan;
   if (p.row_end < 0) p.row_end = p.fact_rows;
-  const uint32_t bpk = (uint32_t)p.bf_bits_per_key;
+  const bool bf_auto = p.bf_bits_per_key == SJ_BF_AUTO;
+  const uint32_t bpk = bf_auto ? 0u : (uint32_t)p.bf_bits_per_key;  // auto: sized as the direct bitmap
   default_geom(eng, &p, q->geom, q->rows_per_thread);
   if (p.tune.compact_threshold) { /* compaction rounds always use full CTAs */ }
   st = check_geom(eng, q->geom, q->rows_per_thread);
@@ -383,9 +384,9 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
     R.payload_min = D.payload_min;
     R.payload_span = D.group ? (uint32_t)((int64_t)D.payload_max - D.payload_min + 1) : 0u;
     R.grouped = D.group ? 1u : 0u;
-    R.bf_mode = bpk ? kBfBlocked : kBfDirect;
-    R.bf_k = bpk ? (uint32_t)p.bf_hashes : 1u;
-    R.bf_bits_per_key = bpk;
+    R.bf_mode = bf_auto ? kBfAuto : (bpk ? kBfBlocked : kBfDirect);
+    R.bf_k = (bpk || bf_auto) ? (uint32_t)p.bf_hashes : 1u;
+    R.bf_bits_per_key = bf_auto ? kAutoBitsPerKey : bpk;
     R.bf_max_log2 = bf_max_log2[d];
     if (D.pred_kind == SJ_PRED_IN) {
       uint32_t* bm = q->in_bitmaps.data() + d * (SJ_MAX_IN_CODES / 32);
@@ -495,8 +496,8 @@ extern "C" sj_status sj_query_get_stats(sj_query* q, sj_query_stats* out) {
   for (int d = 0; d < q->plan.n_dims; ++d) {
     out->bf_inserted[d] = desc.dim[d].n_inserted;
     const uint32_t l2 = desc.dim[d].bf_log2;
-    out->bf_words[d] = q->rt.dim[d].bf_mode == kBfDirect ? std::max<uint64_t>(2, (1ull << l2) / 32)
-                                                         : (2ull << l2);
+    out->bf_words[d] = desc.dim[d].bf_mode == kBfDirect ? std::max<uint64_t>(2, (1ull << l2) / 32) : (2ull << l2);
+    out->bf_blocked[d] = desc.dim[d].bf_mode == kBfBlocked ? 1 : 0;
   }
   out->groups = desc.groups_out;
   out->reorders = desc.reorders;

@@ -47,7 +47,11 @@ enum : uint32_t {
 enum : uint32_t {
   kBfDirect = 0,   // one bit per PHT slot, 32-bit words (crystal/bloom.cuh layout)
   kBfBlocked = 1,  // k bits inside one 64-bit word per key (register-blocked)
+  kBfAuto = 2,     // plan only: the build picks direct or blocked per dimension
 };
+
+// Bits per inserted key of the blocked filter that kBfAuto falls back to.
+constexpr uint32_t kAutoBitsPerKey = 16;
 
 // Per-dimension state the build kernels compute on the device.
 struct SjDimDev {
@@ -55,6 +59,8 @@ struct SjDimDev {
   uint32_t bf_log2;        // blocked: log2(#64-bit words); direct: log2(#bits)
   uint32_t n_codes;        // distinct payload values of qualifying rows (grouped dims)
   uint32_t group_stride;   // multiplier of the dim's code in the group index
+  uint32_t bf_mode;        // layout the build wrote (kBfDirect or kBfBlocked)
+  uint32_t pad_;
 };
 
 // Per-query device descriptor (build writes, probe/finalize read, host fetches).
@@ -196,6 +202,27 @@ __host__ __device__ __forceinline__ uint32_t bf_blocked_log2(uint64_t n_inserted
   if (words < 1) words = 1;
   uint32_t l = ceil_log2(words);
   return l > max_log2 ? max_log2 : l;
+}
+
+// Filter layout and size of one dimension once its qualifying rows are counted.
+// kBfDirect: one bit per PHT slot (log2 = bf_max_log2 bits).  kBfBlocked:
+// words sized from the inserted keys.  kBfAuto: the direct bitmap while it fits
+// the probe's shared-memory filter budget, else the blocked layout at
+// kAutoBitsPerKey bits per inserted key when that is smaller than the direct
+// bitmap (the allocation is the direct bitmap's, so it always fits).
+__host__ __device__ __forceinline__ uint32_t bf_effective(uint32_t mode, uint32_t max_log2, uint32_t bits_per_key,
+                                                          uint32_t n_inserted, uint32_t smem_budget, uint32_t* log2) {
+  if (mode == kBfBlocked) {
+    *log2 = bf_blocked_log2(n_inserted, bits_per_key, max_log2);
+    return kBfBlocked;
+  }
+  *log2 = max_log2;
+  const uint32_t direct_bytes = max_log2 >= 6 ? (1u << max_log2) / 8u : 8u;
+  if (mode == kBfDirect || direct_bytes <= smem_budget || max_log2 < 7) return kBfDirect;
+  const uint32_t bl = bf_blocked_log2(n_inserted, kAutoBitsPerKey, max_log2 - 6);
+  if ((8u << bl) >= direct_bytes) return kBfDirect;
+  *log2 = bl;
+  return kBfBlocked;
 }
 
 }  // namespace sj

@@ -47,6 +47,7 @@ struct Ctl {
   uint32_t stage_ver[16];
   uint32_t bf_in_smem[kMaxDims];  // byte offset within the filter region, or ~0u
   uint32_t bf_log2[kMaxDims];
+  uint32_t bf_mode[kMaxDims];     // layout each dimension's filter was built in
   uint32_t group_stride[kMaxDims];
   uint32_t n_groups;
   uint32_t groups_in_smem;
@@ -146,13 +147,14 @@ __device__ __forceinline__ bool bf_test(const BfView& f, uint32_t slot, uint64_t
 // still matter (grouped dimensions need the code; the direct bitmap is exact over
 // PHT slots, so an ungrouped dimension that has one needs no PHT probe).  Naive:
 // PHT probes only, in join order (src/ssb-jo/q33/0-naive.cu:50-72).
-__device__ inline uint32_t make_steps(const SjPlanRt& P, const uint32_t* order, uint32_t* steps) {
+__device__ inline uint32_t make_steps(const SjPlanRt& P, const uint32_t* bf_mode, const uint32_t* order,
+                                      uint32_t* steps) {
   uint32_t n = 0;
   if (P.lip) {
     for (uint32_t p = 0; p < P.n_dims; ++p) steps[n++] = order[p] | (kStepBF << 4);
     for (uint32_t p = 0; p < P.n_dims; ++p) {
       const SjDimRt& D = P.dim[order[p]];
-      if (D.grouped || D.bf_mode != kBfDirect) steps[n++] = order[p] | (kStepPHT << 4);
+      if (D.grouped || bf_mode[order[p]] != kBfDirect) steps[n++] = order[p] | (kStepPHT << 4);
     }
   } else {
     for (uint32_t p = 0; p < P.n_dims; ++p) steps[n++] = order[p] | (kStepPHT << 4);
@@ -218,7 +220,7 @@ struct Warp {
   __device__ __forceinline__ BfView bfview(uint32_t d) const {
     BfView f;
     const SjDimRt& D = P.dim[d];
-    f.mode = D.bf_mode;
+    f.mode = c.bf_mode[d];
     f.k = D.bf_k;
     f.log2 = c.bf_log2[d];
     f.gptr = D.bf;
@@ -470,7 +472,10 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
   // ---- setup (thread 0): plan steps, filter placement, mbarriers ----------
   if (tid == 0) {
     memset(&c, 0, sizeof(Ctl));
-    for (uint32_t d = 0; d < P.n_dims; ++d) c.bf_log2[d] = desc->dim[d].bf_log2;
+    for (uint32_t d = 0; d < P.n_dims; ++d) {
+      c.bf_log2[d] = desc->dim[d].bf_log2;
+      c.bf_mode[d] = desc->dim[d].bf_mode;
+    }
     // starting order and filter placement, chosen once per query by sj_dim_insert
     uint32_t ord[kMaxDims];
     for (uint32_t d = 0; d < kMaxDims; ++d) {
@@ -478,7 +483,7 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
       c.bf_in_smem[d] = desc->bf_smem_off[d];
     }
     for (uint32_t d = 0; d < kMaxDims; ++d) c.order[0][d] = c.order[1][d] = (d < P.n_dims) ? ord[d] : 0u;
-    c.n_steps[0] = c.n_steps[1] = make_steps(P, ord, c.steps[0]);
+    c.n_steps[0] = c.n_steps[1] = make_steps(P, c.bf_mode, ord, c.steps[0]);
     for (uint32_t p = 0; p < kMaxSteps; ++p) c.steps[1][p] = c.steps[0][p];
     for (uint32_t d = 0; d < P.n_dims; ++d) c.group_stride[d] = desc->dim[d].group_stride;
     c.n_groups = desc->n_groups;
@@ -495,7 +500,7 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
   for (uint32_t d = 0; d < P.n_dims; ++d) {
     if (c.bf_in_smem[d] == ~0u) continue;
     const SjDimRt& D = P.dim[d];
-    const uint32_t bytes = (D.bf_mode == kBfDirect) ? max(8u, (1u << c.bf_log2[d]) / 8u) : (8u << c.bf_log2[d]);
+    const uint32_t bytes = (c.bf_mode[d] == kBfDirect) ? max(8u, (1u << c.bf_log2[d]) / 8u) : (8u << c.bf_log2[d]);
     if (bytes >= 16u) {
       const uint4* src = reinterpret_cast<const uint4*>(D.bf);
       uint4* dst = reinterpret_cast<uint4*>(bfmem + c.bf_in_smem[d]);
@@ -557,7 +562,7 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
           if (order_cost(rate, weight, cand, P.n_dims) < 0.9f * order_cost(rate, weight, cur, P.n_dims)) {
             const uint32_t nv = issue_ver ^ 1u;
             for (uint32_t d = 0; d < kMaxDims; ++d) c.order[nv][d] = (d < P.n_dims) ? cand[d] : 0u;
-            c.n_steps[nv] = make_steps(P, c.order[nv], c.steps[nv]);
+            c.n_steps[nv] = make_steps(P, c.bf_mode, c.order[nv], c.steps[nv]);
             issue_ver = nv;
             last_switch = it;
             c.reorders++;

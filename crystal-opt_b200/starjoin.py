@@ -20,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libstarjoin.so")
 
 MAX_DIMS = 4
+BF_AUTO = -1  # plan.bf_bits_per_key: filter layout chosen per dimension (SJ_BF_AUTO)
 MAX_IN_CODES = 4096
 
 SJ_OK = 0
@@ -96,7 +97,7 @@ class SjQueryStats(C.Structure):
         ("rows_scanned", C.c_uint64), ("step_in", C.c_uint64 * 8), ("step_out", C.c_uint64 * 8),
         ("bf_inserted", C.c_uint64 * MAX_DIMS), ("bf_words", C.c_uint64 * MAX_DIMS),
         ("groups", C.c_uint64), ("reorders", C.c_uint64), ("error_flags", C.c_uint32),
-        ("build_ms", C.c_float), ("probe_ms", C.c_float),
+        ("build_ms", C.c_float), ("probe_ms", C.c_float), ("bf_blocked", C.c_int32 * MAX_DIMS),
     ]
 
 
@@ -467,6 +468,37 @@ def q43_query(schema: StarSchema, order=(0, 1, 2, 3), lip=False, bf_bits_per_key
             _dim("fk_part", "p_key", "p_category", ("in", [3]), "p_brand1", (0, 999), schema.part_rows),
             _date_dim(("range", 1997, 1998))]
     return _shape(dims, schema, order, lip, bf_bits_per_key, bf_hashes, adaptive, sub="supplycost")
+
+
+SSB_SHAPES = {21: q21_query, 22: q22_query, 23: q23_query, 31: q31_query, 32: q32_query, 33: q33_query,
+              34: q34_query, 41: q41_query, 42: q42_query, 43: q43_query}
+
+
+def _int32(v: int) -> int:
+    return ((v + 2 ** 31) % 2 ** 32) - 2 ** 31
+
+
+def ssb_printed(query: int, rows: List[tuple]) -> List[tuple]:
+    """Result tuples (Engine.run / oracle order) in the order the reference's
+    drivers print their groups (the result loops of src/ssb-jo/q*/ drivers):
+    Q2.x (d_year, p_brand1, uint64 sum); Q3.1 (d_year, c_nation, s_nation, uint64
+    sum); Q3.2 / Q3.3 / Q3.4 (d_year, c_city, s_city, int32 sum); Q4.1 (d_year,
+    c_nation, uint64 sum); Q4.2 (d_year, s_nation, p_category, uint64 sum); Q4.3
+    (d_year, s_city, p_brand1, int32 sum).  Drivers that accumulate in int32
+    print the low 32 bits of the sum as a signed value."""
+    if query in (21, 22, 23):
+        return sorted((y, b, v) for (b, y, c, v) in rows)
+    if query == 31:
+        return sorted((y, cn, sn, v) for (cn, sn, y, c, v) in rows)
+    if query in (32, 33, 34):
+        return sorted((y, cc, sc, _int32(v)) for (sc, cc, y, c, v) in rows)
+    if query == 41:
+        return sorted((y, cn, v) for (cn, y, c, v) in rows)
+    if query == 42:
+        return sorted((y, sn, cat, v) for (sn, cat, y, c, v) in rows)
+    if query == 43:
+        return sorted((y, sc, b, _int32(v)) for (sc, b, y, c, v) in rows)
+    raise ValueError(f"no SSB shape {query}")
 
 
 def fill_plan(query: Dict[str, Any], cols: Dict[str, Any], fact_rows: int, tune: Optional[dict] = None):

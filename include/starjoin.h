@@ -48,6 +48,7 @@ extern "C" {
 #define SJ_MAX_DIMS 4
 #define SJ_MAX_IN_CODES 4096   /* IN-list predicates: codes in [0, 4096) */
 #define SJ_MAX_PAYLOAD_SPAN 65536 /* payload_max - payload_min + 1 for grouped dims */
+#define SJ_BF_AUTO (-1)          /* sj_plan.bf_bits_per_key: filter layout chosen per dimension */
 
 typedef enum sj_status {
   SJ_OK = 0,
@@ -115,7 +116,11 @@ typedef struct sj_plan {
   int32_t adaptive;               /* 1: re-rank the LIP order from observed pass rates */
   int32_t bf_bits_per_key;        /* 0: direct bitmap, one bit per key slot
                                      (crystal/bloom.cuh layout); >0: register-blocked
-                                     filter with this many bits per inserted key */
+                                     filter with this many bits per inserted key;
+                                     SJ_BF_AUTO: per dimension, the direct bitmap while it
+                                     fits the probe's shared-memory filter budget, else the
+                                     blocked filter at 16 bits per inserted key (bf_hashes
+                                     bits set) when that is smaller */
   int32_t bf_hashes;              /* blocked filter: bits set per key in one 64-bit word (1..4) */
   sj_tuning tune;
 } sj_plan;
@@ -142,6 +147,7 @@ typedef struct sj_query_stats {
   uint64_t reorders;                   /* adaptive LIP re-rankings (all CTAs) */
   uint32_t error_flags;                /* device-side error bits (0 = none) */
   float build_ms, probe_ms;            /* CUDA-event times of the last run */
+  int32_t bf_blocked[SJ_MAX_DIMS];     /* 1: the dimension's filter was built blocked, 0: direct */
 } sj_query_stats;
 
 typedef struct sj_engine sj_engine;
@@ -216,8 +222,9 @@ const char* sj_noalloc_last_error(void);
 
 /* ---- autotuner ----------------------------------------------------------
  * Chooses the probe's launch geometry (threads per CTA, rows per lane, rows per
- * stage, stage count) and, when asked, the filter kind (direct bitmap or
- * blocked Bloom filter with 4/8/16 bits per key and 1..4 bits set per key) and
+ * stage, stage count) and, when asked, the filter kind (direct bitmap,
+ * SJ_BF_AUTO with 2 or 3 bits set per key, or blocked Bloom filter with 4/8/16
+ * bits per key and 1..4 bits set per key) and
  * the join order, by timing candidates on the plan's own columns (coordinate
  * descent: filter, then geometry, then order).  Every candidate's groups must
  * equal the first candidate's, bit for bit.  With a cache file, the winner is

@@ -5,7 +5,9 @@
 // seeded synthetic columns the engine's tests use (SSB's nested codes derived as
 // nation = city / 10, region = city / 50, category = brand / 40,
 // mfgr = brand / 200, d_yearmonthnum = datekey / 100) and calls the driver's
-// own runQuery(), which prints one line per group.  REF_QUERY selects the driver.
+// own runQuery(), which prints one line per group, --t times (each followed by a
+// {"query":Q,"time_query":ms} line: the driver's own timing of allocations,
+// memsets, builds and probe).  REF_QUERY selects the driver.
 #define main crystal_reference_driver_main
 #include REF_DRIVER
 #undef main
@@ -41,8 +43,9 @@ static int* to_gpu(std::vector<int>& h, long long n) { return loadToGPU<int>(h.d
 int main(int argc, char** argv) {
   CommandLineArgs args(argc, argv);
   unsigned long long seed = 1;
-  int n = 6000000, c_len = 30000, s_len = 2000, p_len = 200000;
+  int n = 6000000, c_len = 30000, s_len = 2000, p_len = 200000, trials = 1;
   args.GetCmdLineArgument("seed", seed);
+  args.GetCmdLineArgument("t", trials);
   args.GetCmdLineArgument("n", n);
   args.GetCmdLineArgument("c", c_len);
   args.GetCmdLineArgument("s", s_len);
@@ -84,16 +87,24 @@ int main(int argc, char** argv) {
   int* p_category = to_gpu(h_p_category, p_len);
   CubDebugExit(cudaDeviceSynchronize());
   fflush(stdout);
-  runQuery(lo_orderdate, lo_partkey, lo_suppkey, lo_revenue, n, p_partkey, p_brand1, p_category, p_len, d_datekey,
+  for (int t = 0; t < trials; ++t) {
+    const float tq = runQuery(lo_orderdate, lo_partkey, lo_suppkey, lo_revenue, n, p_partkey, p_brand1, p_category, p_len, d_datekey,
            d_year, d_len, s_suppkey, s_region, s_len, g_allocator);
+    printf("{\"query\":%d,\"time_query\":%.6f}\n", REF_QUERY, tq);
+    fflush(stdout);
+  }
 #elif REF_QUERY == 22 || REF_QUERY == 23
   int* lo_partkey = to_gpu(h_lo_partkey, n);
   int* p_partkey = to_gpu(h_p_partkey, p_len);
   int* p_brand1 = to_gpu(h_p_brand1, p_len);
   CubDebugExit(cudaDeviceSynchronize());
   fflush(stdout);
-  runQuery(lo_orderdate, lo_partkey, lo_suppkey, lo_revenue, n, p_partkey, p_brand1, p_len, d_datekey, d_year, d_len,
+  for (int t = 0; t < trials; ++t) {
+    const float tq = runQuery(lo_orderdate, lo_partkey, lo_suppkey, lo_revenue, n, p_partkey, p_brand1, p_len, d_datekey, d_year, d_len,
            s_suppkey, s_region, s_len, g_allocator);
+    printf("{\"query\":%d,\"time_query\":%.6f}\n", REF_QUERY, tq);
+    fflush(stdout);
+  }
 #elif REF_QUERY == 32
   int* lo_custkey = to_gpu(h_lo_custkey, n);
   int* s_nation = to_gpu(h_s_nation, s_len);
@@ -103,8 +114,12 @@ int main(int argc, char** argv) {
   int* c_city = to_gpu(h_c_city, c_len);
   CubDebugExit(cudaDeviceSynchronize());
   fflush(stdout);
-  runQuery(lo_orderdate, lo_custkey, lo_suppkey, lo_revenue, n, d_datekey, d_year, d_len, s_suppkey, s_nation,
+  for (int t = 0; t < trials; ++t) {
+    const float tq = runQuery(lo_orderdate, lo_custkey, lo_suppkey, lo_revenue, n, d_datekey, d_year, d_len, s_suppkey, s_nation,
            s_city, s_len, c_custkey, c_nation, c_city, c_len, g_allocator);
+    printf("{\"query\":%d,\"time_query\":%.6f}\n", REF_QUERY, tq);
+    fflush(stdout);
+  }
 #elif REF_QUERY == 34
   int* lo_custkey = to_gpu(h_lo_custkey, n);
   int* d_yearmonthnum = to_gpu(h_d_yearmonthnum, d_len);
@@ -113,8 +128,12 @@ int main(int argc, char** argv) {
   int* c_city = to_gpu(h_c_city, c_len);
   CubDebugExit(cudaDeviceSynchronize());
   fflush(stdout);
-  runQuery(lo_orderdate, lo_custkey, lo_suppkey, lo_revenue, n, d_datekey, d_year, d_yearmonthnum, d_len,
+  for (int t = 0; t < trials; ++t) {
+    const float tq = runQuery(lo_orderdate, lo_custkey, lo_suppkey, lo_revenue, n, d_datekey, d_year, d_yearmonthnum, d_len,
            s_suppkey, s_city, s_len, c_custkey, c_city, c_len, g_allocator);
+    printf("{\"query\":%d,\"time_query\":%.6f}\n", REF_QUERY, tq);
+    fflush(stdout);
+  }
 #elif REF_QUERY == 31
   int* lo_custkey = to_gpu(h_lo_custkey, n);
   int* s_nation = to_gpu(h_s_nation, s_len);
@@ -123,8 +142,12 @@ int main(int argc, char** argv) {
   int* c_nation = to_gpu(h_c_nation, c_len);
   CubDebugExit(cudaDeviceSynchronize());
   fflush(stdout);
-  runQuery(lo_orderdate, lo_custkey, lo_suppkey, lo_revenue, n, d_datekey, d_year, d_len, s_suppkey, s_region,
+  for (int t = 0; t < trials; ++t) {
+    const float tq = runQuery(lo_orderdate, lo_custkey, lo_suppkey, lo_revenue, n, d_datekey, d_year, d_len, s_suppkey, s_region,
            s_nation, s_len, c_custkey, c_region, c_nation, c_len, g_allocator);
+    printf("{\"query\":%d,\"time_query\":%.6f}\n", REF_QUERY, tq);
+    fflush(stdout);
+  }
 #elif REF_QUERY == 41
   int* lo_custkey = to_gpu(h_lo_custkey, n);
   int* lo_partkey = to_gpu(h_lo_partkey, n);
@@ -136,8 +159,12 @@ int main(int argc, char** argv) {
   int* c_nation = to_gpu(h_c_nation, c_len);
   CubDebugExit(cudaDeviceSynchronize());
   fflush(stdout);
-  runQuery(lo_orderdate, lo_custkey, lo_partkey, lo_suppkey, lo_revenue, lo_supplycost, n, d_datekey, d_year, d_len,
+  for (int t = 0; t < trials; ++t) {
+    const float tq = runQuery(lo_orderdate, lo_custkey, lo_partkey, lo_suppkey, lo_revenue, lo_supplycost, n, d_datekey, d_year, d_len,
            p_partkey, p_mfgr, p_len, s_suppkey, s_region, s_len, c_custkey, c_region, c_nation, c_len, g_allocator);
+    printf("{\"query\":%d,\"time_query\":%.6f}\n", REF_QUERY, tq);
+    fflush(stdout);
+  }
 #elif REF_QUERY == 42
   int* lo_custkey = to_gpu(h_lo_custkey, n);
   int* lo_partkey = to_gpu(h_lo_partkey, n);
@@ -150,9 +177,13 @@ int main(int argc, char** argv) {
   int* c_region = to_gpu(h_c_region, c_len);
   CubDebugExit(cudaDeviceSynchronize());
   fflush(stdout);
-  runQuery(lo_orderdate, lo_custkey, lo_partkey, lo_suppkey, lo_revenue, lo_supplycost, n, d_datekey, d_year, d_len,
+  for (int t = 0; t < trials; ++t) {
+    const float tq = runQuery(lo_orderdate, lo_custkey, lo_partkey, lo_suppkey, lo_revenue, lo_supplycost, n, d_datekey, d_year, d_len,
            p_partkey, p_mfgr, p_category, p_len, s_suppkey, s_region, s_nation, s_len, c_custkey, c_region, c_len,
            g_allocator);
+    printf("{\"query\":%d,\"time_query\":%.6f}\n", REF_QUERY, tq);
+    fflush(stdout);
+  }
 #elif REF_QUERY == 43
   int* lo_custkey = to_gpu(h_lo_custkey, n);
   int* lo_partkey = to_gpu(h_lo_partkey, n);
@@ -166,9 +197,13 @@ int main(int argc, char** argv) {
   int* c_region = to_gpu(h_c_region, c_len);
   CubDebugExit(cudaDeviceSynchronize());
   fflush(stdout);
-  runQuery(lo_orderdate, lo_custkey, lo_partkey, lo_suppkey, lo_revenue, lo_supplycost, n, d_datekey, d_year, d_len,
+  for (int t = 0; t < trials; ++t) {
+    const float tq = runQuery(lo_orderdate, lo_custkey, lo_partkey, lo_suppkey, lo_revenue, lo_supplycost, n, d_datekey, d_year, d_len,
            p_partkey, p_category, p_brand1, p_len, s_suppkey, s_nation, s_city, s_len, c_custkey, c_region, c_len,
            g_allocator);
+    printf("{\"query\":%d,\"time_query\":%.6f}\n", REF_QUERY, tq);
+    fflush(stdout);
+  }
 #else
 #error "REF_QUERY must be 21, 22, 23, 31, 32, 34, 41, 42 or 43"
 #endif

@@ -28,7 +28,8 @@ def test_shape_matches_oracle(sj, oracle, engine, shapes, query):
     orders = list(itertools.permutations(range(n)))[:: max(1, len(list(itertools.permutations(range(n)))) // 4)]
     for order in orders:
         for lip, bpk, k, adaptive in ((True, 0, 2, False), (True, 8, 3, True), (True, 16, 2, False),
-                                      (False, 0, 2, False)):
+                                      (False, 0, 2, False), (True, sj.BF_AUTO, 2, False),
+                                      (True, sj.BF_AUTO, 3, True)):
             q = make(SHAPES_SMALL, order=order, lip=lip, bf_bits_per_key=bpk, bf_hashes=k, adaptive=adaptive)
             got, _ = engine.run(q, dev, SHAPES_SMALL.fact_rows)
             assert got == want, (query, order, lip, bpk, k, adaptive)
@@ -80,3 +81,23 @@ def test_ssb_shapes_in_one_shared_scan(sj, oracle, engine, shapes):
             b.close()
         for p, g in zip(plain, got):
             assert g == oracle.run(p, host)
+
+
+def test_auto_filter_layout_per_dimension(sj, oracle, engine, shapes):
+    """bf_bits_per_key = BF_AUTO with a 16 KB filter budget: Q2.3's part
+    dimension (p_brand1 == 260, about 200 of 200,000 keys; a 32 KB direct
+    bitmap over 2^18 slots) gets the blocked layout, the supplier (256 B) and
+    date (8 KB) bitmaps stay direct, and the groups equal the oracle's."""
+    host, dev = shapes
+    q = sj.q23_query(SHAPES_SMALL, bf_bits_per_key=sj.BF_AUTO)
+    pq = engine.prepare(q, dev, SHAPES_SMALL.fact_rows, tune={"bf_smem_bytes": 16384})
+    try:
+        pq.build()
+        pq.probe()
+        got = pq.fetch()
+        st = pq.stats()
+    finally:
+        pq.release()
+    assert got == oracle.run(q, host)
+    assert list(st.bf_blocked)[:3] == [0, 1, 0]
+    assert st.bf_words[1] * 4 < 32768 // 4  # blocked: 1,000 keys x 16 bits, far below the direct bitmap

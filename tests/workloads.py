@@ -31,31 +31,7 @@ SHAPE_QUERIES = {21: sj.q21_query, 22: sj.q22_query, 23: sj.q23_query, 31: sj.q3
 SHAPE_WIDTH = {21: 3, 22: 3, 23: 3, 31: 4, 32: 4, 34: 4, 41: 3, 42: 4, 43: 4}
 
 
-def _int32(v: int) -> int:
-    return ((v + 2 ** 31) % 2 ** 32) - 2 ** 31
-
-
-def shape_as_printed(query: int, rows: List[tuple]) -> List[tuple]:
-    """Engine / oracle result tuples in the order the reference drivers print
-    them (the result loops of src/ssb-jo/q*/ drivers):
-    Q2.x (d_year, p_brand1, uint64 sum); Q3.1 (d_year, c_nation, s_nation, uint64
-    sum); Q3.2 / Q3.4 (d_year, c_city, s_city, int32 sum); Q4.1 (d_year, c_nation,
-    uint64 sum); Q4.2 (d_year, s_nation, p_category, uint64 sum); Q4.3 (d_year,
-    s_city, p_brand1, int32 sum).  Drivers that accumulate in int32 print the
-    low 32 bits of the sum as a signed value."""
-    if query in (21, 22, 23):
-        return sorted((y, b, v) for (b, y, c, v) in rows)
-    if query == 31:
-        return sorted((y, cn, sn, v) for (cn, sn, y, c, v) in rows)
-    if query in (32, 34):
-        return sorted((y, cc, sc, _int32(v)) for (sc, cc, y, c, v) in rows)
-    if query == 41:
-        return sorted((y, cn, v) for (cn, y, c, v) in rows)
-    if query == 42:
-        return sorted((y, sn, cat, v) for (sn, cat, y, c, v) in rows)
-    if query == 43:
-        return sorted((y, sc, b, _int32(v)) for (sc, b, y, c, v) in rows)
-    raise ValueError(f"no shape {query}")
+shape_as_printed = sj.ssb_printed  # result tuples in the order the reference drivers print them
 
 
 FOURDIM = sj.StarSchema(seed=0x5EED0003, fact_rows=120_000_000, cust_rows=600_000, supp_rows=40_000,
