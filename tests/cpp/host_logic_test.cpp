@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "sj_cache.h"
+#include "sj_internal.h"
 
 using namespace sj;
 
@@ -263,7 +264,29 @@ static void test_perms() {
   }
 }
 
+// Filter layout of one dimension once its qualifying rows are counted (the
+// per-dimension choice of bf_bits_per_key = SJ_BF_AUTO).
+static void test_bf_effective() {
+  uint32_t l2 = 99;
+  // explicit modes are kept
+  CHECK(bf_effective(kBfDirect, 20, 0, 100, 40960, &l2) == kBfDirect && l2 == 20);
+  CHECK(bf_effective(kBfBlocked, 20, 8, 1000, 40960, &l2) == kBfBlocked && l2 == bf_blocked_log2(1000, 8, 20));
+  // auto: a direct bitmap that fits the budget stays direct (2^16 bits = 8 KB)
+  CHECK(bf_effective(kBfAuto, 16, 16, 40000, 40960, &l2) == kBfDirect && l2 == 16);
+  // auto: 2^20 bits = 128 KB over the budget, 1,000 keys x 16 bits -> 256 words of 64 bits
+  CHECK(bf_effective(kBfAuto, 20, 16, 1000, 40960, &l2) == kBfBlocked && l2 == 8);
+  // auto: blocked would not be smaller than the direct bitmap -> direct
+  CHECK(bf_effective(kBfAuto, 20, 16, 65536, 40960, &l2) == kBfDirect && l2 == 20);
+  // auto: no qualifying key -> one 64-bit word (rejects every row)
+  CHECK(bf_effective(kBfAuto, 20, 16, 0, 40960, &l2) == kBfBlocked && l2 == 0);
+  // the blocked filter always fits the direct bitmap's allocation
+  for (uint32_t lg = 7; lg <= 28; ++lg)
+    for (uint32_t ins : {0u, 1u, 100u, 5000u, 1u << 20, 1u << 26})
+      if (bf_effective(kBfAuto, lg, 16, ins, 0, &l2) == kBfBlocked) CHECK((8ull << l2) < (1ull << lg) / 8);
+}
+
 int main() {
+  test_bf_effective();
   test_perms();
   test_range_alloc();
   test_filter_cache();
