@@ -212,6 +212,7 @@ struct Warp {
   unsigned long long* s_sum;
   uint32_t* s_cnt;
   uint32_t bf_base;
+  const uint8_t* bf_ptr;  // the same filter region as a shared-memory pointer
   uint64_t base_row;
   uint64_t pol_first, pol_keep;
   uint32_t lane;
@@ -361,11 +362,16 @@ struct Warp {
   // Per lane and pass: RPL independent rows; the pass bits collect in a register
   // mask, and one warp prefix scan of the mask popcounts places the survivors.
   template <int RPL, int MODE, int K, bool FULL>
-  __device__ __forceinline__ uint32_t scan(uint32_t ver, uint32_t sbuf, const First& f, uint32_t off, uint32_t rows,
-                                           uint64_t cstart, uint32_t crows, uint32_t tma_rows, uint32_t skip,
-                                           uint32_t rel0, const int32_t* pf) {
+  __device__ __forceinline__ uint32_t scan(uint32_t ver, const int32_t* sbuf, const First& f, uint32_t off,
+                                           uint32_t rows, uint64_t cstart, uint32_t crows, uint32_t tma_rows,
+                                           uint32_t skip, uint32_t rel0, const int32_t* pf) {
     static_assert(RPL <= 32, "pass mask is 32 bits");
     const uint32_t t_begin = t1;
+    // plain shared-memory loads (not volatile asm), so the compiler can schedule a
+    // pass's staged loads and filter lookups together; the mbarrier waits and
+    // arrives around a stage carry memory clobbers
+    const uint8_t* fbase = (MODE == kModeDirectSmem || MODE == kModeBlockedSmem) ? bf_ptr + (f.bf.smem - bf_base)
+                                                                                  : nullptr;
     for (uint32_t i0 = off; i0 < off + rows; i0 += 32u * RPL) {
       uint32_t d[RPL];
       uint32_t valid = ~0u;  // bit j: row j of this lane lies in the scanned range
@@ -373,7 +379,7 @@ struct Warp {
 #pragma unroll
       for (uint32_t j4 = 0; j4 < RPL / 4; ++j4) {
         const uint32_t r4 = i0 + (j4 * 32u + lane) * 4u;
-        const int4 v = lds_v4(sbuf + r4 * 4u);
+        const int4 v = *reinterpret_cast<const int4*>(sbuf + r4);
         int32_t fk[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (uint32_t j = 0; j < 4; ++j) {
@@ -398,12 +404,12 @@ struct Warp {
         const uint32_t sl = d[j];
         bool ok;
         if (MODE == kModeDirectSmem) {
-          const uint32_t wd = lds_u32(f.bf.smem + (sl >> 5) * 4u);
+          const uint32_t wd = reinterpret_cast<const uint32_t*>(fbase)[sl >> 5];
           ok = __funnelshift_r(wd, wd, sl) & 1u;  // rotate right: bit (sl mod 32) to bit 0
         } else if (MODE == kModeBlockedSmem) {
           const uint32_t h1 = bf_h1(sl);
           const uint32_t w = __funnelshift_rc(h1, 0u, 32u - f.bf.log2);  // h1 >> (32 - log2), 0 for log2 = 0
-          const uint2 wv = lds_u32x2(f.bf.smem + w * 8u);
+          const uint2 wv = reinterpret_cast<const uint2*>(fbase)[w];
           ok = bf_test_word<K>(wv.x, wv.y, bf_g(h1));
         } else if (MODE == kModeBfAny) {
           ok = bf_test(f.bf, sl, pol_keep);
@@ -594,7 +600,7 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
     Warp w{P, c,
            reinterpret_cast<uint32_t*>(smem + L.q1_off) + warp * G.q1_cap,
            reinterpret_cast<uint32_t*>(smem + L.q2_off) + warp * G.q2_cap,
-           G.q1_cap - 1, G.q2_cap - 1, s_sum, s_cnt, smem_addr(bfmem), base_row, pol_first, pol_keep, lane,
+           G.q1_cap - 1, G.q2_cap - 1, s_sum, s_cnt, smem_addr(bfmem), bfmem, base_row, pol_first, pol_keep, lane,
            0, 0, 0, 0};
     const uint32_t slice = CH / NWC;
     const uint32_t my_off = warp * slice;
@@ -640,7 +646,7 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
         const uint32_t d1 = c.steps[ver][1] & 15u;
         if (d1 != d0) pf = P.dim[d1].fact_fk + base_row;
       }
-      const uint32_t sbuf = smem_addr(stage + (size_t)s * CH);
+      const int32_t* sbuf = stage + (size_t)s * CH;
       const bool fullc = (crows == CH) && (skip == 0);
       uint32_t passed;
 #define SJ_SCAN(M, K)                                                                                            \
