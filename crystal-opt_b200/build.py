@@ -18,7 +18,7 @@ LIB = os.path.join(BUILD, "libstarjoin.so")
 
 SOURCES = ["sj_engine.cu", "sj_build.cu", "sj_probe.cu", "sj_batch.cu", "sj_batch_host.cu", "sj_serve.cu",
            "sj_autotune.cu", "sj_ssbio.cu", "sj_noalloc.cu"]
-HEADERS = ["sj_internal.h", "sj_ptx.cuh", "sj_datagen.h", "sj_shared.h", "sj_cache.h"]
+HEADERS = ["sj_internal.h", "sj_ptx.cuh", "sj_datagen.h", "sj_shared.h", "sj_cache.h", "sj_l2.h"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-pthread"]
 

@@ -623,20 +623,20 @@ uint32_t sjb_probe_smem_bytes(uint32_t smem_entries) {
 
 template <int NW, bool PF>
 static cudaError_t launch_probe_nw(const SjbSchemaRt& S, const SjbStep* step, SjbAcc* acc, SjbCounters* ctr,
-                                   uint32_t smem_entries, int sm_count, cudaStream_t st) {
+                                   uint32_t smem_entries, int sm_count, cudaStream_t st, const L2Window& w) {
   const uint32_t smem = sjb_probe_smem_bytes(smem_entries);
   cudaError_t e = cudaFuncSetAttribute(sjb_probe_kernel<NW, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  sjb_probe_kernel<NW, PF><<<sm_count, NW * 32, smem, st>>>(S, step, acc, ctr);
-  return cudaGetLastError();
+  return launch_windowed(sjb_probe_kernel<NW, PF>, dim3(sm_count), dim3(NW * 32), smem, st, w, S, step, acc, ctr);
 }
 
 cudaError_t sjb_launch_probe(const SjbSchemaRt& S, const SjbStep* step, SjbAcc* acc, SjbCounters* ctr,
-                             uint32_t threads, uint32_t smem_entries, int sm_count, cudaStream_t st) {
+                             uint32_t threads, uint32_t smem_entries, int sm_count, cudaStream_t st,
+                             const L2Window& w) {
   switch (threads) {
-    case 256: return launch_probe_nw<8, true>(S, step, acc, ctr, smem_entries, sm_count, st);
-    case 512: return launch_probe_nw<16, true>(S, step, acc, ctr, smem_entries, sm_count, st);
-    case 1024: return launch_probe_nw<32, false>(S, step, acc, ctr, smem_entries, sm_count, st);
+    case 256: return launch_probe_nw<8, true>(S, step, acc, ctr, smem_entries, sm_count, st, w);
+    case 512: return launch_probe_nw<16, true>(S, step, acc, ctr, smem_entries, sm_count, st, w);
+    case 1024: return launch_probe_nw<32, false>(S, step, acc, ctr, smem_entries, sm_count, st, w);
   }
   return cudaErrorInvalidValue;
 }

@@ -86,6 +86,7 @@ sj_status schema_register(sj_engine* eng, const sjb_schema* sc, SchemaState& st)
   R.fact_rows = sc->fact_rows;
   SJB_CUDA(cudaSetDevice(eng->device));
   SJB_CUDA(cudaMalloc(&st.masks, std::max<uint64_t>(total_len, 1) * sizeof(uint64_t)));
+  st.masks_bytes = std::max<uint64_t>(total_len, 1) * sizeof(uint64_t);
   SJB_CUDA(cudaMalloc(&st.slot_attr, std::max<uint64_t>(total_attr, 1) * sizeof(int32_t)));
   SJB_CUDA(cudaMemset(st.masks, 0, std::max<uint64_t>(total_len, 1) * sizeof(uint64_t)));
   SJB_CUDA(cudaMemset(st.slot_attr, 0, std::max<uint64_t>(total_attr, 1) * sizeof(int32_t)));
@@ -342,7 +343,8 @@ static cudaError_t batch_enqueue(sjb_batch* b, cudaStream_t st) {
   SJB_Q(sjb_launch_zero_groups(b->step_d, ~0ull, b->acc, sm, st));
   SJB_Q(sjb_launch_compose(b->S.rt, b->step_d, sm, st));
   SJB_Q(cudaEventRecordWithFlags(b->ev[1], st, b->lim.use_graph ? cudaEventRecordExternal : cudaEventRecordDefault));
-  SJB_Q(sjb_launch_probe(b->S.rt, b->step_d, b->acc, b->ctr_d, b->threads, b->smem_entries, sm, st));
+  SJB_Q(sjb_launch_probe(b->S.rt, b->step_d, b->acc, b->ctr_d, b->threads, b->smem_entries, sm, st,
+                         l2_window(b->S.masks, b->S.masks_bytes, b->eng->l2_persist_bytes, b->eng->l2_window_max)));
   SJB_Q(cudaEventRecordWithFlags(b->ev[2], st, b->lim.use_graph ? cudaEventRecordExternal : cudaEventRecordDefault));
   SJB_Q(sjb_launch_finalize(b->step_d, ~0ull, b->acc, b->rows_d, (uint64_t)b->lim.result_rows, b->ctr_d, nullptr,
                             sm, st));

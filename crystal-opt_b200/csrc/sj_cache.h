@@ -291,6 +291,7 @@ struct SchemaState {
   sjb_schema schema{};
   SjbSchemaRt rt{};
   uint64_t* masks = nullptr;      // all dimensions' 64-bit slot words
+  size_t masks_bytes = 0;
   int32_t* slot_attr = nullptr;   // all dimensions' slot-attribute tables
   int64_t attr_min[SJ_MAX_DIMS][SJB_MAX_ATTRS]{};
   int64_t attr_max[SJ_MAX_DIMS][SJB_MAX_ATTRS]{};

@@ -23,7 +23,8 @@
 
 namespace sj {
 uint32_t probe_smem_bytes(const SjProbeGeom& g);
-cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_per_thread, cudaStream_t st);
+cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_per_thread, cudaStream_t st,
+                         const L2Window& w);
 cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st);
 __global__ void sj_dim_scan(const __grid_constant__ SjPlanRt P);
 __global__ void sj_dim_insert(const __grid_constant__ SjPlanRt P);
@@ -84,6 +85,54 @@ sj_status set_error(sj_status s, const char* msg) {
 
 // ---------------------------------------------------------------- engine ----
 
+// Persisting-L2 set-aside for the probes' access-policy windows, shared by every
+// engine of this process on a device: the first engine reserves it (at most
+// kL2PersistWant, within the device maximum) and the last one gives the
+// previous limit back.  The limit belongs to this process's CUDA context; where
+// it cannot be changed (MPS, MIG) the probes launch without windows.
+namespace {
+#ifndef SJ_L2_PERSIST_MB
+#define SJ_L2_PERSIST_MB 48
+#endif
+constexpr size_t kL2PersistWant = (size_t)SJ_L2_PERSIST_MB << 20;
+std::mutex g_l2_mu;
+struct L2Reservation {
+  int users = 0;
+  size_t prev = 0, held = 0;
+};
+L2Reservation g_l2[64];
+
+size_t l2_acquire(int device) {
+  std::lock_guard<std::mutex> g(g_l2_mu);
+  L2Reservation& r = g_l2[device & 63];
+  if (r.users++ == 0) {
+    int max_persist = 0;
+    r.held = 0;
+    if (cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, device) == cudaSuccess &&
+        max_persist > 0 && cudaDeviceGetLimit(&r.prev, cudaLimitPersistingL2CacheSize) == cudaSuccess) {
+      const size_t want = std::min<size_t>(kL2PersistWant, (size_t)max_persist);
+      if (want > r.prev && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess) r.held = want;
+      else if (r.prev > 0) r.held = r.prev;  // an existing set-aside is used as it is
+    }
+    cudaGetLastError();
+  }
+  return r.held;
+}
+
+void l2_release(int device) {
+  std::lock_guard<std::mutex> g(g_l2_mu);
+  L2Reservation& r = g_l2[device & 63];
+  if (r.users > 0 && --r.users == 0) {
+    if (r.held && r.held != r.prev) {
+      cudaCtxResetPersistingL2Cache();
+      cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, r.prev);
+    }
+    r.held = 0;
+    cudaGetLastError();
+  }
+}
+}  // namespace
+
 extern "C" sj_status sj_engine_create(int device, sj_engine** out) {
   if (!out) return fail(SJ_ERR_INVALID_ARGUMENT, "out is NULL");
   *out = nullptr;
@@ -103,6 +152,7 @@ extern "C" sj_status sj_engine_create(int device, sj_engine** out) {
   eng->device = device;
   eng->sm_count = prop.multiProcessorCount;
   eng->smem_optin = prop.sharedMemPerBlockOptin;
+  eng->l2_window_max = prop.accessPolicyMaxWindowSize > 0 ? (size_t)prop.accessPolicyMaxWindowSize : 0;
   cudaMemPoolProps pp;
   memset(&pp, 0, sizeof(pp));
   pp.allocType = cudaMemAllocationTypePinned;
@@ -122,6 +172,7 @@ extern "C" sj_status sj_engine_create(int device, sj_engine** out) {
     delete eng;
     return fail(SJ_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
   }
+  eng->l2_persist_bytes = l2_acquire(device);
   *out = eng;
   return SJ_OK;
 }
@@ -132,6 +183,7 @@ extern "C" void sj_engine_destroy(sj_engine* e) {
   cudaDeviceSynchronize();
   if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
   if (e->pool) cudaMemPoolDestroy(e->pool);
+  l2_release(e->device);
   delete e;
 }
 
@@ -152,6 +204,7 @@ struct sj_query {
   cudaEvent_t ev_start = nullptr, ev_built = nullptr, ev_probed = nullptr;
   bool built = false, probed = false;
   cudaStream_t stream = nullptr;
+  L2Window l2win;  // the probe's window over the hash tables and filters
 };
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -344,6 +397,9 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
                 q->arena_bytes, cudaGetErrorString(e));
   }
 
+  // hash tables, filters and payload bitmaps lie in [ht_off[0], gsum_off) of the arena
+  q->l2win = l2_window(q->arena + ht_off[0], gsum_off - ht_off[0], eng->l2_persist_bytes, eng->l2_window_max);
+
   // ---- runtime parameters
   SjPlanRt& rt = q->rt;
   memset(&rt, 0, sizeof(rt));
@@ -442,7 +498,7 @@ extern "C" sj_status sj_query_probe(sj_query* q, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   SJ_CUDA(cudaSetDevice(q->eng->device));
   if (q->rt.row_end > q->rt.row_begin) {
-    SJ_CUDA(launch_probe(q->rt, q->geom, q->rows_per_thread, st));
+    SJ_CUDA(launch_probe(q->rt, q->geom, q->rows_per_thread, st, q->l2win));
   }
   SJ_CUDA(launch_finalize(q->rt, (uint32_t)q->group_capacity, st));
   SJ_CUDA(cudaEventRecord(q->ev_probed, st));
@@ -624,7 +680,7 @@ static sj_status run_query_streamed(sj_engine* eng, sj_plan p, const int32_t* ho
       SjPlanRt rt = q->rt;
       rt.row_begin = (uint64_t)std::max<int64_t>(pb, b);
       rt.row_end = (uint64_t)pe;
-      if (ce == cudaSuccess) ce = launch_probe(rt, q->geom, q->rows_per_thread, st);
+      if (ce == cudaSuccess) ce = launch_probe(rt, q->geom, q->rows_per_thread, st, q->l2win);
       if (ce != cudaSuccess) s = fail(SJ_ERR_CUDA, "streamed probe: %s", cudaGetErrorString(ce));
       pb = pe;
     }

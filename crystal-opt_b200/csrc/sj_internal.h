@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
+#include "sj_l2.h"
+
 // Named range on the host timeline for each stage (NVTX v3, header-only: free
 // unless a profiler is attached).
 struct SjNvtxRange {
@@ -24,6 +26,8 @@ struct sj_engine {
   size_t smem_optin = 232448;
   cudaMemPool_t pool = nullptr;
   cudaStream_t copy_stream = nullptr;  // host->device staging of streamed columns
+  size_t l2_persist_bytes = 0;         // persisting-L2 set-aside held for the probes (0: none)
+  size_t l2_window_max = 0;            // largest access-policy window the device takes
 };
 
 namespace sj {

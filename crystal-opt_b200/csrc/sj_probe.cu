@@ -735,19 +735,21 @@ __global__ void __launch_bounds__(256) sj_finalize_kernel(const __grid_constant_
 uint32_t probe_smem_bytes(const SjProbeGeom& g) { return probe_layout(g).total; }
 
 template <int NWC, int RPL>
-static cudaError_t launch_probe_t(const SjPlanRt& P, const SjProbeGeom& G, uint32_t smem, cudaStream_t st) {
+static cudaError_t launch_probe_t(const SjPlanRt& P, const SjProbeGeom& G, uint32_t smem, cudaStream_t st,
+                                  const L2Window& w) {
   cudaError_t e = cudaFuncSetAttribute(sj_probe_kernel<NWC, RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  sj_probe_kernel<NWC, RPL><<<G.grid, (NWC + 1) * 32, smem, st>>>(P, G);
-  return cudaGetLastError();
+  return launch_windowed(sj_probe_kernel<NWC, RPL>, dim3(G.grid), dim3((NWC + 1) * 32), smem, st, w, P, G);
 }
 
-// G.threads = 32 * (consumer warps + 1); rows_per_lane: rows each lane tests per pass.
-cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_per_lane, cudaStream_t st) {
+// G.threads = 32 * (consumer warps + 1); rows_per_lane: rows each lane tests per pass;
+// w: L2 window over the query's hash tables and filters (may be empty).
+cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_per_lane, cudaStream_t st,
+                         const L2Window& w) {
   const uint32_t smem = probe_layout(G).total;
   const uint32_t nwc = G.threads / 32 - 1;
 #define SJ_CASE(W, R) \
-  if (nwc == W && rows_per_lane == R) return launch_probe_t<W, R>(P, G, smem, st);
+  if (nwc == W && rows_per_lane == R) return launch_probe_t<W, R>(P, G, smem, st, w);
   SJ_CASE(7, 8)
   SJ_CASE(7, 16)
   SJ_CASE(15, 8)

@@ -461,7 +461,8 @@ bool launch_step(sjs_server* s, bool* launched) {
     if (cudaMemsetAsync(ctr, 0, 2 * sizeof(SjbCounters), s->st) != cudaSuccess) return false;
     const uint32_t threads = s->cfg.limits.threads ? (uint32_t)s->cfg.limits.threads : 1024u;
     if (cudaEventRecord(s->ev_probe[b][0], s->st) != cudaSuccess) return false;
-    if (sjb_launch_probe(s->S.rt, s->step_d, s->acc, ctr, threads, st.smem_entries, s->eng->sm_count, s->st) !=
+    const L2Window w = l2_window(s->S.masks, s->S.masks_bytes, s->eng->l2_persist_bytes, s->eng->l2_window_max);
+    if (sjb_launch_probe(s->S.rt, s->step_d, s->acc, ctr, threads, st.smem_entries, s->eng->sm_count, s->st, w) !=
         cudaSuccess)
       return false;
     if (cudaEventRecord(s->ev_probe[b][1], s->st) != cudaSuccess) return false;

@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "sj_l2.h"
+
 #include "../../include/starjoin_batch.h"
 
 namespace sj {
@@ -288,7 +290,8 @@ cudaError_t sjb_launch_zero_groups(const SjbStep* step, uint64_t zero_mask, SjbA
                                    cudaStream_t st);
 cudaError_t sjb_launch_compose(const SjbSchemaRt& S, const SjbStep* step, int sm_count, cudaStream_t st);
 cudaError_t sjb_launch_probe(const SjbSchemaRt& S, const SjbStep* step, SjbAcc* acc, SjbCounters* ctr,
-                             uint32_t threads, uint32_t smem_entries, int sm_count, cudaStream_t st);
+                             uint32_t threads, uint32_t smem_entries, int sm_count, cudaStream_t st,
+                             const L2Window& masks_window);
 cudaError_t sjb_launch_finalize(const SjbStep* step, uint64_t mask, const SjbAcc* acc, sjb_row* out,
                                 uint64_t cap, SjbCounters* ctr, const int32_t* slot_query, int sm_count,
                                 cudaStream_t st);

@@ -3,6 +3,7 @@ groups, counts and uint64 sums, for every join order, naive and LIP, each filter
 layout, and the edge cases the reference's kernels meet (ragged tiles, key == len,
 empty inputs)."""
 import ctypes as C
+import os
 import random
 
 import numpy as np
@@ -290,3 +291,40 @@ def test_adaptive_lip_reorders_when_the_estimate_misleads(sj, engine, full, torc
     fixed = sj.q33_query(FULL, order=(1, 0, 2), bf_bits_per_key=16, adaptive=False)
     _, _, want = _probe_ms(engine, fixed, cols, n, reps=1)
     assert got == want
+
+
+def test_l2_set_aside_reserved_and_given_back(torch_cuda):
+    """The engine reserves a persisting-L2 set-aside for the probes'
+    access-policy windows while it lives and puts the previous limit back when
+    the last engine of the process goes (checked in a fresh process, through
+    the CUDA runtime's own cudaDeviceGetLimit)."""
+    import subprocess
+    import sys
+    code = r'''
+import ctypes, os, sys
+sys.path.insert(0, os.path.join(sys.argv[1], "crystal-opt_b200"))
+import nvidia.cuda_runtime
+import starjoin as sj
+rt = ctypes.CDLL(os.path.join(os.path.dirname(nvidia.cuda_runtime.__file__), "lib", "libcudart.so.12"))
+lim = ctypes.c_size_t()
+def get():
+    assert rt.cudaDeviceGetLimit(ctypes.byref(lim), 6) == 0  # cudaLimitPersistingL2CacheSize
+    return lim.value
+rt.cudaFree(None)
+before = get()
+a = sj.Engine(0)
+during = get()
+b = sj.Engine(0)
+a.close()
+still = get()
+b.close()
+after = get()
+print(before, during, still, after)
+'''
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code, root], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    before, during, still, after = map(int, out.stdout.split())
+    assert during >= before and during > 0
+    assert still == during  # a second engine keeps the set-aside
+    assert after == before
