@@ -433,6 +433,10 @@ def main():
     ap.add_argument("--shapes", action="store_true",
                     help="run only the SSB query shapes (Q2.1-Q4.3) at 120M rows: this engine, or with "
                          "--impl reference the reference's own CUDA drivers on the same schema")
+    ap.add_argument("--queries", default="",
+                    help="--shapes: comma-separated SSB query numbers (e.g. 41,43); default all ten")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="--shapes: skip the plan search (reference join order, LIP, automatic filter layout)")
     args = ap.parse_args()
     FACT_ROWS = args.rows
     args.warmup = max(3, args.warmup)
@@ -459,20 +463,25 @@ def run_shapes(args):
     reference's own unmodified CUDA drivers (oracle/_ref) on the same seeded
     schema with their `time_query`; groups_sha1 digests compare the two."""
     import shapes_bench
+    schema = dict(shapes_bench.SCHEMA)
+    if args.rows != 120_000_000:
+        schema["fact_rows"] = args.rows
+    queries = tuple(int(x) for x in args.queries.split(",") if x) or shapes_bench.QUERIES
     if args.impl != "reference":
         import starjoin as sj
         eng = sj.Engine(0)
-        print(json.dumps({"shapes": shapes_bench.shapes(eng, reps=max(3, min(args.steps, 20)))}), flush=True)
+        print(json.dumps({"shapes": shapes_bench.shapes(eng, reps=max(3, min(args.steps, 20)), schema=schema,
+                                                        queries=queries, autotune=not args.no_autotune)}), flush=True)
         eng.close()
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import build_ref
-    sc = shapes_bench.SCHEMA
+    sc = schema
     width = {21: 3, 22: 3, 23: 3, 31: 4, 32: 4, 33: 4, 34: 4, 41: 3, 42: 4, 43: 4}
     trials = max(3, min(args.steps, 10))
     out = {"impl": "reference", "workload": "SSB query shapes, reference CUDA drivers (unmodified, sm_100a)",
            "queries": {}}
-    for q in shapes_bench.QUERIES:
+    for q in queries:
         exe = build_ref.binary(0, "lip") if q == 33 else build_ref.shape_binary(q)
         if not os.path.exists(exe):
             out["queries"][str(q)] = {"unavailable": "oracle/_ref not built"}

@@ -40,7 +40,11 @@ def _fact_bytes_per_row(q: Dict[str, Any]) -> int:
     return 4 * (len(q["dims"]) + 1 + (1 if q.get("measure_sub") else 0))
 
 
-def shapes(eng: sj.Engine, reps: int = 10, schema: Dict[str, int] = None, queries=QUERIES) -> Dict[str, Any]:
+def shapes(eng: sj.Engine, reps: int = 10, schema: Dict[str, int] = None, queries=QUERIES,
+           autotune: bool = True) -> Dict[str, Any]:
+    """autotune=False runs the reference's join order with LIP, the per-dimension
+    automatic filter layout and adaptive re-ranking, without the plan search
+    (small profiling runs)."""
     import torch
     sc = sj.StarSchema(**(schema or SCHEMA))
     cols = sj.gen_device(sc)
@@ -68,8 +72,12 @@ def shapes(eng: sj.Engine, reps: int = 10, schema: Dict[str, int] = None, querie
     for qn in queries:
         ref_plan = sj.SSB_SHAPES[qn](sc)
         q0 = dict(ref_plan, lip=True)
-        q, tune, rep = eng.autotune(q0, cols, sc.fact_rows, reps=3, tune_filter=True, tune_order=2, verify=True,
-                                    stream=sp)
+        if autotune:
+            q, tune, rep = eng.autotune(q0, cols, sc.fact_rows, reps=3, tune_filter=True, tune_order=2, verify=True,
+                                        stream=sp)
+            candidates = rep.candidates
+        else:
+            q, tune, candidates = dict(q0, bf_bits_per_key=sj.BF_AUTO, adaptive=True), {}, 0
         rows, _ = eng.run(q, cols, sc.fact_rows, tune=tune, stream=sp)
         ref_rows, _ = eng.run(ref_plan, cols, sc.fact_rows, stream=sp)
         times = []
@@ -85,7 +93,7 @@ def shapes(eng: sj.Engine, reps: int = 10, schema: Dict[str, int] = None, querie
             "probe_ms_reference_plan": probe_ms(ref_plan, None),
             "plan": {"order": q["order"], "lip": q["lip"], "bf_bits_per_key": q["bf_bits_per_key"],
                      "bf_hashes": q["bf_hashes"], "threads": tune.get("threads", 0),
-                     "autotune_candidates": rep.candidates},
+                     "autotune_candidates": candidates},
             "same_as_reference_plan": rows == ref_rows,
             "groups": len(printed), "groups_sha1": groups_digest(printed),
         }
