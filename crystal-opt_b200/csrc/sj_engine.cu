@@ -297,7 +297,7 @@ static void default_geom(sj_engine* eng, const sj_plan* p, SjProbeGeom& g, uint3
   uint32_t q1 = 1;
   while (q1 < 2 * 32 * rpl) q1 <<= 1;
   g.q1_cap = q1;
-  g.q2_cap = 64;
+  g.q2_cap = 128;  // room for a two-survivors-per-lane Q1 round (64) over a partial Q2
   g.reorder_period = 16;
   const uint32_t per_sm = t.ctas_per_sm ? (uint32_t)t.ctas_per_sm : 1u;
   g.grid = (uint32_t)eng->sm_count * per_sm;

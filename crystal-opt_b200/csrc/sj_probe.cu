@@ -203,6 +203,9 @@ struct First {
 };
 
 // State of one consumer warp.  Every field is identical in all 32 lanes.
+// PAIR: Q1 rounds may take two survivors per lane (q1_pair); off where the
+// CTA's register budget has no room for the second survivor's state.
+template <bool PAIR>
 struct Warp {
   const SjPlanRt& P;
   Ctl& c;
@@ -337,6 +340,50 @@ struct Warp {
     h1 += cnt;
   }
 
+  // Q1 entries [h1, h1 + 64) of a plan with more than two steps: q1_round on
+  // two survivors per lane, with both lanes' step-1 loads (the next FK column,
+  // then its filter word or PHT slot) in flight together, the survivors queued
+  // in Q2.  The caller leaves 64 free Q2 entries.
+  __device__ __forceinline__ void q1_pair(uint32_t ver) {
+    __syncwarp();
+    const uint32_t st1 = c.steps[ver][1];
+    const uint32_t d1 = st1 & 15u;
+    const bool bf1 = (st1 >> 4) == kStepBF;
+    const uint32_t ra = q1[(h1 + lane) & q1m], rb = q1[(h1 + 32u + lane) & q1m];
+    const uint32_t s_a = slot_at(d1, ra), s_b = slot_at(d1, rb);
+    bool pa, pb;
+    if (bf1) {
+      const BfView f = bfview(d1);
+      pa = bf_test(f, s_a, pol_keep);
+      pb = bf_test(f, s_b, pol_keep);
+    } else {
+      pa = ld_slot(P.dim[d1].ht + s_a, pol_keep).x != 0;
+      pb = ld_slot(P.dim[d1].ht + s_b, pol_keep).x != 0;
+    }
+    const uint32_t ma = __ballot_sync(0xffffffffu, pa), mb = __ballot_sync(0xffffffffu, pb);
+    const uint32_t d2 = c.steps[ver][2] & 15u;
+    if (pa) {
+      q2[(t2 + __popc(ma & lanemask_lt())) & q2m] = ra;
+      if (d2 != d1) prefetch_l2(P.dim[d2].fact_fk + base_row + ra);
+    }
+    t2 += __popc(ma);
+    if (pb) {
+      q2[(t2 + __popc(mb & lanemask_lt())) & q2m] = rb;
+      if (d2 != d1) prefetch_l2(P.dim[d2].fact_fk + base_row + rb);
+    }
+    t2 += __popc(mb);
+    if (lane == 0) {
+      const uint32_t out = (uint32_t)(__popc(ma) + __popc(mb));
+      atomicAdd(&c.step_in[1], 64u);
+      atomicAdd(&c.step_out[1], out);
+      if (bf1) {
+        atomicAdd(&c.probes[d1], 64u);
+        atomicAdd(&c.passes[d1], out);
+      }
+    }
+    h1 += 64;
+  }
+
   __device__ __forceinline__ void q2_round(uint32_t ver, uint32_t cnt) {
     __syncwarp();
     if (lane < cnt) finish(ver, 2, q2[(h2 + lane) & q2m], 0u, 0u, Vals4{0, 0, 0, 0}, Vals4{0, 0, 0, 0});
@@ -349,6 +396,8 @@ struct Warp {
       const uint32_t a1 = t1 - h1, a2 = t2 - h2;
       if (a2 >= 32 || (drain && a2 > 0 && a1 == 0)) {
         q2_round(ver, min(a2, 32u));
+      } else if (PAIR && a1 >= 64 && a2 + 64u <= q2m + 1u && c.n_steps[ver] > 2) {
+        q1_pair(ver);
       } else if (a1 >= 32 || (drain && a1 > 0)) {
         q1_round(ver, min(a1, 32u));
       } else {
@@ -597,7 +646,7 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
     }
   } else {
     // ---- consumer warps ------------------------------------------------------
-    Warp w{P, c,
+    Warp<(NWC <= 15)> w{P, c,
            reinterpret_cast<uint32_t*>(smem + L.q1_off) + warp * G.q1_cap,
            reinterpret_cast<uint32_t*>(smem + L.q2_off) + warp * G.q2_cap,
            G.q1_cap - 1, G.q2_cap - 1, s_sum, s_cnt, smem_addr(bfmem), bfmem, base_row, pol_first, pol_keep, lane,
@@ -649,9 +698,12 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
       const int32_t* sbuf = stage + (size_t)s * CH;
       const bool fullc = (crows == CH) && (skip == 0);
       uint32_t passed;
-#define SJ_SCAN(M, K)                                                                                            \
-  passed = fullc ? w.scan<RPL, M, K, true>(ver, sbuf, f, my_off, slice, cstart, crows, tma_rows, skip, rel0, pf) \
-                 : w.scan<RPL, M, K, false>(ver, sbuf, f, my_off, slice, cstart, crows, tma_rows, skip, rel0, pf)
+#define SJ_SCAN(M, K)                                                                                        \
+  passed = fullc                                                                                             \
+               ? w.template scan<RPL, M, K, true>(ver, sbuf, f, my_off, slice, cstart, crows, tma_rows, skip, \
+                                                  rel0, pf)                                                   \
+               : w.template scan<RPL, M, K, false>(ver, sbuf, f, my_off, slice, cstart, crows, tma_rows, skip, \
+                                                   rel0, pf)
       if (mode == kModeDirectSmem) SJ_SCAN(kModeDirectSmem, 0);
       else if (mode == kModeBlockedSmem) {
         if (f.bf.k == 1) SJ_SCAN(kModeBlockedSmem, 1);
