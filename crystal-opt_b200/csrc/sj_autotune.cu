@@ -3,10 +3,12 @@
 // Candidates are timed on the plan's own device columns with CUDA events around
 // sj_query_probe (the build is re-run before every timed probe, as a query
 // would).  Search order, each step keeping the best so far:
-//   1. filter kind   direct bitmap, per-dimension auto layout (x 2..3 bits set),
-//                    or 4 / 8 / 16 bits per key x 1..4 bits set
+//   1. filter kind   direct bitmap, per-dimension auto layout, 8 or 16 bits per
+//                    key -- with every join order when the order is searched too
 //   2. geometry      threads x rows per lane, then rows per stage x stages
-//   3. join order    most selective first, or every permutation
+//   3. join order    (when not searched in 1) most selective first, or every
+//                    permutation; then bits set per key 1..4 and 4 / 8 / 16
+//                    bits per key for the chosen order and geometry
 // The groups of every candidate are compared with the first candidate's.
 #include <cuda_runtime.h>
 
@@ -207,19 +209,32 @@ extern "C" sj_status sj_autotune(sj_engine* eng, sj_plan* plan, const sj_autotun
       best = c;
     }
   };
-  // 1. filter kind
+  // 1. filter kind, jointly with the join order when both are searched: a
+  //    large, selective dimension pays off first in the order only with a
+  //    filter that fits shared memory, so neither choice is right alone
+  auto for_orders = [&](const sj_plan& base, bool all_orders) {
+    if (!all_orders || cur.n_dims < 2) {
+      consider(base);
+      return;
+    }
+    int perm[SJ_MAX_DIMS];
+    for (int i = 0; i < cur.n_dims; ++i) perm[i] = i;
+    do {
+      sj_plan c = base;
+      for (int i = 0; i < cur.n_dims; ++i) c.order[i] = perm[i];
+      consider(c);
+    } while (std::next_permutation(perm, perm + cur.n_dims));
+  };
+  const bool joint = o.tune_filter && o.tune_order == 2;
   if (o.tune_filter) {
     const sj_plan start = best;
-    const int bpks[] = {0, SJ_BF_AUTO, 4, 8, 16};
-    for (int bpk : bpks)
-      for (int k = 1; k <= (bpk > 0 ? 4 : (bpk < 0 ? 3 : 1)); ++k) {
-        if (bpk < 0 && k == 1) continue;  // auto: 2 or 3 bits per key where it goes blocked
-        sj_plan c = start;
-        c.bf_bits_per_key = bpk;
-        c.bf_hashes = bpk ? k : 2;
-        if (c.bf_bits_per_key == start.bf_bits_per_key && (bpk == 0 || c.bf_hashes == start.bf_hashes)) continue;
-        consider(c);
-      }
+    const int kinds[][2] = {{0, 2}, {SJ_BF_AUTO, 2}, {SJ_BF_AUTO, 3}, {8, 2}, {16, 2}};
+    for (auto& kd : kinds) {
+      sj_plan c = start;
+      c.bf_bits_per_key = kd[0];
+      c.bf_hashes = kd[1];
+      for_orders(c, joint);
+    }
   }
   // 2. geometry: CTA size x rows per lane, then rows per stage x stages
   {
@@ -251,20 +266,21 @@ extern "C" sj_status sj_autotune(sj_engine* eng, sj_plan* plan, const sj_autotun
         consider(c);
       }
   }
-  // 3. join order
-  if (o.tune_order == 2 && cur.n_dims > 1) {
+  // 3. join order (when not searched with the filter), then bits set per key
+  //    and the other filter sizes for the chosen order and geometry
+  if (o.tune_order == 2 && !joint && cur.n_dims > 1) for_orders(best, true);
+  if (o.tune_filter) {
     const sj_plan start = best;
-    int perm[SJ_MAX_DIMS];
-    for (int i = 0; i < cur.n_dims; ++i) perm[i] = i;
-    do {
-      sj_plan c = start;
-      bool same = true;
-      for (int i = 0; i < cur.n_dims; ++i) {
-        c.order[i] = perm[i];
-        same = same && perm[i] == start.order[i];
+    const int bpks[] = {SJ_BF_AUTO, 4, 8, 16};
+    for (int bpk : bpks)
+      for (int k = 1; k <= (bpk > 0 ? 4 : 3); ++k) {
+        if (bpk < 0 && k == 1) continue;
+        if (bpk == start.bf_bits_per_key && k == start.bf_hashes) continue;
+        sj_plan c = start;
+        c.bf_bits_per_key = bpk;
+        c.bf_hashes = k;
+        consider(c);
       }
-      if (!same) consider(c);
-    } while (std::next_permutation(perm, perm + cur.n_dims));
   }
   rep.best_ms = best_ms;
   *plan = best;
