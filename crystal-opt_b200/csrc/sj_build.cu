@@ -55,28 +55,29 @@ __global__ void __launch_bounds__(256) sj_dim_scan(const __grid_constant__ SjPla
   if (lane == 0 && count) atomicAdd(&desc->dim[d].n_inserted, count);
 }
 
-// Block-wide exclusive scan of popcounts of `words` bitmap words into pre[].
+// Exclusive prefix of the popcounts of `words` bitmap words into pre[] (and their
+// total), by warp 0 with shuffles: payload bitmaps are at most 2,048 words
+// (SJ_MAX_PAYLOAD_SPAN bits), 1-32 for the SSB attributes.  One block barrier.
 __device__ void bitmap_prefix(const uint32_t* bm, uint32_t words, uint32_t* pre, uint32_t* total) {
-  __shared__ uint32_t part[256];
-  const uint32_t t = threadIdx.x, nt = blockDim.x;
-  const uint32_t per = (words + nt - 1) / nt;
-  const uint32_t b = t * per, e = min(words, b + per);
-  uint32_t s = 0;
-  for (uint32_t w = b; w < e; ++w) s += __popc(bm[w]);
-  part[t] = s;
-  __syncthreads();
-  for (uint32_t off = 1; off < nt; off <<= 1) {
-    uint32_t v = (t >= off) ? part[t - off] : 0u;
-    __syncthreads();
-    part[t] += v;
-    __syncthreads();
+  if (threadIdx.x < 32) {
+    const uint32_t lane = threadIdx.x;
+    const uint32_t per = (words + 31) / 32;
+    const uint32_t b = lane * per, e = min(words, b + per);
+    uint32_t s = 0;
+    for (uint32_t w = b; w < e; ++w) s += __popc(bm[w]);
+    uint32_t incl = s;
+#pragma unroll
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    uint32_t run = incl - s;  // exclusive
+    for (uint32_t w = b; w < e; ++w) {
+      pre[w] = run;
+      run += __popc(bm[w]);
+    }
+    if (total && lane == 31) *total = incl;
   }
-  uint32_t run = part[t] - s;  // exclusive
-  for (uint32_t w = b; w < e; ++w) {
-    pre[w] = run;
-    run += __popc(bm[w]);
-  }
-  if (total && t == nt - 1) *total = part[t];
   __syncthreads();
 }
 
