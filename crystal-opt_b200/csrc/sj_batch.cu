@@ -627,7 +627,8 @@ static cudaError_t launch_probe_nw(const SjbSchemaRt& S, const SjbStep* step, Sj
   const uint32_t smem = sjb_probe_smem_bytes(smem_entries);
   cudaError_t e = cudaFuncSetAttribute(sjb_probe_kernel<NW, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  return launch_windowed(sjb_probe_kernel<NW, PF>, dim3(sm_count), dim3(NW * 32), smem, st, w, S, step, acc, ctr);
+  return launch_windowed(sjb_probe_kernel<NW, PF>, dim3(sm_count), dim3(NW * 32), smem, st, w, false, S, step, acc,
+                         ctr);
 }
 
 cudaError_t sjb_launch_probe(const SjbSchemaRt& S, const SjbStep* step, SjbAcc* acc, SjbCounters* ctr,

@@ -31,6 +31,7 @@ __device__ __forceinline__ bool dim_pred(const SjDimRt& D, uint64_t i) {
 }
 
 __global__ void __launch_bounds__(256) sj_dim_scan(const __grid_constant__ SjPlanRt P) {
+  pdl_launch_dependents();  // sj_dim_insert may be scheduled; it waits for this grid
   const uint32_t d = blockIdx.y;
   if (d >= P.n_dims) return;
   const SjDimRt& D = P.dim[d];
@@ -155,6 +156,8 @@ __device__ void choose_start(const SjPlanRt& P, SjDesc* desc) {
 }
 
 __global__ void __launch_bounds__(256) sj_dim_insert(const __grid_constant__ SjPlanRt P) {
+  pdl_launch_dependents();  // the probe may be scheduled; it waits for this grid
+  pdl_wait();               // sj_dim_scan's counts and payload bitmaps are complete
   extern __shared__ uint32_t prefix[];  // payload-bitmap prefix popcounts
   __shared__ uint32_t s_total;
   const uint32_t d = blockIdx.y;

@@ -24,8 +24,8 @@
 namespace sj {
 uint32_t probe_smem_bytes(const SjProbeGeom& g);
 cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_per_thread, cudaStream_t st,
-                         const L2Window& w);
-cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st);
+                         const L2Window& w, bool pdl);
+cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st, bool pdl);
 __global__ void sj_dim_scan(const __grid_constant__ SjPlanRt P);
 __global__ void sj_dim_insert(const __grid_constant__ SjPlanRt P);
 }  // namespace sj
@@ -483,8 +483,7 @@ extern "C" sj_status sj_query_build(sj_query* q, void* stream) {
   dim3 grid(bx, (unsigned)q->plan.n_dims);
   sj_dim_scan<<<grid, 256, 0, st>>>(q->rt);
   SJ_CUDA(cudaGetLastError());
-  sj_dim_insert<<<grid, 256, 4 * max_pwords, st>>>(q->rt);
-  SJ_CUDA(cudaGetLastError());
+  SJ_CUDA(launch_windowed(sj_dim_insert, grid, dim3(256), 4 * max_pwords, st, L2Window{}, true, q->rt));
   SJ_CUDA(cudaEventRecord(q->ev_built, st));
   q->built = true;
   q->stream = st;
@@ -498,9 +497,9 @@ extern "C" sj_status sj_query_probe(sj_query* q, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   SJ_CUDA(cudaSetDevice(q->eng->device));
   if (q->rt.row_end > q->rt.row_begin) {
-    SJ_CUDA(launch_probe(q->rt, q->geom, q->rows_per_thread, st, q->l2win));
+    SJ_CUDA(launch_probe(q->rt, q->geom, q->rows_per_thread, st, q->l2win, true));
   }
-  SJ_CUDA(launch_finalize(q->rt, (uint32_t)q->group_capacity, st));
+  SJ_CUDA(launch_finalize(q->rt, (uint32_t)q->group_capacity, st, true));
   SJ_CUDA(cudaEventRecord(q->ev_probed, st));
   q->probed = true;
   q->stream = st;
@@ -680,13 +679,13 @@ static sj_status run_query_streamed(sj_engine* eng, sj_plan p, const int32_t* ho
       SjPlanRt rt = q->rt;
       rt.row_begin = (uint64_t)std::max<int64_t>(pb, b);
       rt.row_end = (uint64_t)pe;
-      if (ce == cudaSuccess) ce = launch_probe(rt, q->geom, q->rows_per_thread, st, q->l2win);
+      if (ce == cudaSuccess) ce = launch_probe(rt, q->geom, q->rows_per_thread, st, q->l2win, false);
       if (ce != cudaSuccess) s = fail(SJ_ERR_CUDA, "streamed probe: %s", cudaGetErrorString(ce));
       pb = pe;
     }
   }
   if (s == SJ_OK) {
-    cudaError_t ce = launch_finalize(q->rt, (uint32_t)q->group_capacity, st);
+    cudaError_t ce = launch_finalize(q->rt, (uint32_t)q->group_capacity, st, false);
     if (ce != cudaSuccess) s = fail(SJ_ERR_CUDA, "finalize: %s", cudaGetErrorString(ce));
     q->built = q->probed = true;
     q->stream = st;

@@ -43,27 +43,37 @@ inline L2Window l2_window(const void* base, size_t bytes, size_t persist_bytes, 
   return w;
 }
 
-// Launch `kernel` with the window as a launch attribute (a plain launch when the
-// window is empty).
+// Launch `kernel` with the window as a launch attribute (none when the window is
+// empty).  pdl: programmatic dependent launch -- the kernel may be scheduled
+// while the previous kernel of the stream runs, and waits (griddepcontrol.wait)
+// for it before reading its output; only for a kernel whose predecessor in the
+// stream is a kernel that calls pdl_launch_dependents.
 template <typename... K, typename... A>
 cudaError_t launch_windowed(void (*kernel)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                            const L2Window& w, A&&... args) {
+                            const L2Window& w, bool pdl, A&&... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
+  unsigned n = 0;
   if (w.bytes) {
-    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
-    attr[0].val.accessPolicyWindow.base_ptr = const_cast<void*>(w.base);
-    attr[0].val.accessPolicyWindow.num_bytes = w.bytes;
-    attr[0].val.accessPolicyWindow.hitRatio = w.hit_ratio;
-    attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-    attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    attr[n].id = cudaLaunchAttributeAccessPolicyWindow;
+    attr[n].val.accessPolicyWindow.base_ptr = const_cast<void*>(w.base);
+    attr[n].val.accessPolicyWindow.num_bytes = w.bytes;
+    attr[n].val.accessPolicyWindow.hitRatio = w.hit_ratio;
+    attr[n].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr[n].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    ++n;
   }
+  if (pdl) {
+    attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[n].val.programmaticStreamSerializationAllowed = 1;
+    ++n;
+  }
+  cfg.attrs = n ? attr : nullptr;
+  cfg.numAttrs = n;
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
 }
 

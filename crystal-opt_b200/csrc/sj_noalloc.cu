@@ -29,8 +29,8 @@
 namespace sj {
 uint32_t probe_smem_bytes(const SjProbeGeom& g);
 cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_per_thread, cudaStream_t st,
-                         const L2Window& w);
-cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st);
+                         const L2Window& w, bool pdl);
+cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st, bool pdl);
 __global__ void sj_dim_scan(const __grid_constant__ SjPlanRt P);
 __global__ void sj_dim_insert(const __grid_constant__ SjPlanRt P);
 }  // namespace sj
@@ -244,8 +244,8 @@ extern "C" sj_status sj_ssb_q33_run_noalloc(int device, const int32_t* lo_orderd
   if ((s = check(cudaGetLastError(), "dimension scan")) != SJ_OK) return s;
   sj_dim_insert<<<grid, 256, 4 * ((250 + 31) / 32), st>>>(rt);
   if ((s = check(cudaGetLastError(), "dimension insert")) != SJ_OK) return s;
-  if (lo_len > 0 && (s = check(launch_probe(rt, g, 8, st, L2Window{}), "probe")) != SJ_OK) return s;
-  if ((s = check(launch_finalize(rt, (uint32_t)groups, st), "finalize")) != SJ_OK) return s;
+  if (lo_len > 0 && (s = check(launch_probe(rt, g, 8, st, L2Window{}, false), "probe")) != SJ_OK) return s;
+  if ((s = check(launch_finalize(rt, (uint32_t)groups, st, false), "finalize")) != SJ_OK) return s;
   SjDesc desc;
   if ((s = check(cudaMemcpyAsync(&desc, rt.desc, sizeof(desc), cudaMemcpyDeviceToHost, st), "reading status")) != SJ_OK)
     return s;

@@ -508,6 +508,8 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
                                                                      const __grid_constant__ SjProbeGeom G) {
   static_assert(RPL % 4 == 0, "rows per lane must be a multiple of 4");
   constexpr uint32_t NT = (NWC + 1) * 32;
+  pdl_launch_dependents();
+  pdl_wait();  // the build's descriptor, hash tables and filters are complete
   extern __shared__ __align__(128) uint8_t smem[];
   const SmemLayout L = probe_layout(G);
   int32_t* stage = reinterpret_cast<int32_t*>(smem + L.stage_off);
@@ -762,6 +764,7 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
 // Compact the non-empty groups into result rows, decoding dictionary codes back
 // to payload values.
 __global__ void __launch_bounds__(256) sj_finalize_kernel(const __grid_constant__ SjPlanRt P) {
+  pdl_wait();  // the probe's group sums are complete
   SjDesc* desc = P.desc;
   const uint32_t n_groups = desc->n_groups;
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < n_groups; g += gridDim.x * blockDim.x) {
@@ -788,20 +791,22 @@ uint32_t probe_smem_bytes(const SjProbeGeom& g) { return probe_layout(g).total; 
 
 template <int NWC, int RPL>
 static cudaError_t launch_probe_t(const SjPlanRt& P, const SjProbeGeom& G, uint32_t smem, cudaStream_t st,
-                                  const L2Window& w) {
+                                  const L2Window& w, bool pdl) {
   cudaError_t e = cudaFuncSetAttribute(sj_probe_kernel<NWC, RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  return launch_windowed(sj_probe_kernel<NWC, RPL>, dim3(G.grid), dim3((NWC + 1) * 32), smem, st, w, P, G);
+  return launch_windowed(sj_probe_kernel<NWC, RPL>, dim3(G.grid), dim3((NWC + 1) * 32), smem, st, w, pdl, P, G);
 }
 
 // G.threads = 32 * (consumer warps + 1); rows_per_lane: rows each lane tests per pass;
-// w: L2 window over the query's hash tables and filters (may be empty).
+// w: L2 window over the query's hash tables and filters (may be empty); pdl: the
+// previous kernel of the stream is the build's sj_dim_insert (programmatic
+// dependent launch).
 cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_per_lane, cudaStream_t st,
-                         const L2Window& w) {
+                         const L2Window& w, bool pdl) {
   const uint32_t smem = probe_layout(G).total;
   const uint32_t nwc = G.threads / 32 - 1;
 #define SJ_CASE(W, R) \
-  if (nwc == W && rows_per_lane == R) return launch_probe_t<W, R>(P, G, smem, st, w);
+  if (nwc == W && rows_per_lane == R) return launch_probe_t<W, R>(P, G, smem, st, w, pdl);
   SJ_CASE(7, 8)
   SJ_CASE(7, 16)
   SJ_CASE(15, 8)
@@ -812,12 +817,12 @@ cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st) {
+// pdl: the previous kernel of the stream is the probe (programmatic dependent launch).
+cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st, bool pdl) {
   uint32_t blocks = (group_capacity + 255) / 256;
   if (blocks > 1184) blocks = 1184;
   if (blocks < 1) blocks = 1;
-  sj_finalize_kernel<<<blocks, 256, 0, st>>>(P);
-  return cudaGetLastError();
+  return launch_windowed(sj_finalize_kernel, dim3(blocks), dim3(256), 0, st, L2Window{}, pdl, P);
 }
 
 }  // namespace sj
