@@ -283,13 +283,15 @@ extern "C" sj_status sjb_batch_create(sj_engine* eng, const sjb_schema* schema, 
   if (L.filter_cache_bytes <= 0) L.filter_cache_bytes = 1ll << 30;
   b->threads = L.threads ? (uint32_t)L.threads : 1024u;
   if (b->threads != 256 && b->threads != 512 && b->threads != 1024) {
+    const int threads = L.threads;
     delete b;
-    return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "threads=%d (256, 512 or 1024)", L.threads);
+    return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "threads=%d (256, 512 or 1024)", threads);
   }
   b->smem_entries = L.smem_group_entries > 0 ? (uint32_t)L.smem_group_entries : 6144u;
   if (sjb_probe_smem_bytes(b->smem_entries) + 1024 > eng->smem_optin) {
+    const int entries = L.smem_group_entries;
     delete b;
-    return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "smem_group_entries=%d does not fit shared memory", L.smem_group_entries);
+    return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "smem_group_entries=%d does not fit shared memory", entries);
   }
   b->prefix_rows = std::min<uint64_t>(b->prefix_rows, (uint64_t)L.result_rows);
   sj_status rc = schema_register(eng, schema, b->S);

@@ -392,9 +392,10 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
   cudaError_t e = cudaMallocFromPoolAsync((void**)&q->arena, q->arena_bytes, eng->pool, 0);
   if (e != cudaSuccess) {
     cudaGetLastError();
+    const size_t bytes = q->arena_bytes;
     delete q;
-    return fail(e == cudaErrorMemoryAllocation ? SJ_ERR_OUT_OF_MEMORY : SJ_ERR_CUDA, "query arena of %zu B: %s",
-                q->arena_bytes, cudaGetErrorString(e));
+    return fail(e == cudaErrorMemoryAllocation ? SJ_ERR_OUT_OF_MEMORY : SJ_ERR_CUDA, "query arena of %zu B: %s", bytes,
+                cudaGetErrorString(e));
   }
 
   // hash tables, filters and payload bitmaps lie in [ht_off[0], gsum_off) of the arena
