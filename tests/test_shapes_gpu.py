@@ -101,3 +101,28 @@ def test_auto_filter_layout_per_dimension(sj, oracle, engine, shapes):
     assert got == oracle.run(q, host)
     assert list(st.bf_blocked)[:3] == [0, 1, 0]
     assert st.bf_words[1] * 4 < 32768 // 4  # blocked: 1,000 keys x 16 bits, far below the direct bitmap
+
+
+@pytest.mark.parametrize("codes,expect_blocked", [([], 1), (list(range(25)), 0)])
+def test_auto_filter_edges(sj, oracle, engine, shapes, codes, expect_blocked):
+    """BF_AUTO at its edges, on a part dimension whose direct bitmap (2^18 slots,
+    32 KB) is over a 16 KB budget: a predicate that accepts nothing gets a
+    one-word blocked filter that rejects every row; one that accepts every row
+    keeps the direct bitmap (the blocked one would not be smaller).  Groups equal
+    the oracle's, under adaptive re-ranking too."""
+    host, dev = shapes
+    q = sj.q21_query(SHAPES_SMALL, bf_bits_per_key=sj.BF_AUTO, adaptive=True)
+    q["dims"][1]["pred"] = ("in", codes) if codes else ("range", 1000, 2000)
+    q["dims"][1]["attr"] = "p_category"
+    pq = engine.prepare(q, dev, SHAPES_SMALL.fact_rows, tune={"bf_smem_bytes": 16384})
+    try:
+        pq.build()
+        pq.probe()
+        got = pq.fetch()
+        st = pq.stats()
+    finally:
+        pq.release()
+    want = oracle.run(q, host)
+    assert got == want
+    assert st.bf_blocked[1] == expect_blocked
+    assert (len(want) == 0) == (not codes)
