@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(256) sjb_zero_jobs_kernel(const SjbBatchDesc* 
   const uint32_t j = blockIdx.y;
   if (j >= D->n_jobs) return;
   const SjbJob& J = D->jobs[j];
+  if (J.stats_mask & kJobStatsOnly) return;  // its filter is built and in use
   for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < J.words; w += gridDim.x * blockDim.x)
     J.bitmap[w] = 0u;
   if (blockIdx.x == 0 && threadIdx.x < sizeof(SjbEntryStats) / 4)
@@ -83,7 +84,9 @@ __global__ void __launch_bounds__(256) sjb_zero_jobs_kernel(const SjbBatchDesc* 
 // and attributes are read once, then every job's predicate is evaluated on them
 // (blockIdx.y = dimension).  Per job and warp: one ballot, one atomicOr per
 // distinct bitmap word, and the statistics only when some row qualified, kept
-// in shared memory and flushed once per block.
+// in shared memory and flushed once per block.  The min/max of an attribute is
+// reduced only when the job's stats_mask names it (the attributes its queries
+// group by); statistics-only jobs skip the bitmap and the count.
 constexpr uint32_t kBuildThreads = 256;
 
 __global__ void __launch_bounds__(kBuildThreads) sjb_build_kernel(const __grid_constant__ SjbSchemaRt S,
@@ -152,6 +155,7 @@ __global__ void __launch_bounds__(kBuildThreads) sjb_build_kernel(const __grid_c
       uint32_t pend = __ballot_sync(kFull, ok);
       if (!pend) continue;  // warp-uniform
       const uint32_t n_ok = __popc(pend);
+      if (J.stats_mask & kJobStatsOnly) pend = 0;  // the bitmap is built already
       while (pend) {  // one atomicOr per distinct bitmap word in the warp
         const uint32_t leader = __ffs(pend) - 1u;
         const uint32_t lw = __shfl_sync(kFull, wd, leader);
@@ -163,7 +167,7 @@ __global__ void __launch_bounds__(kBuildThreads) sjb_build_kernel(const __grid_c
       if (lane == 0) atomicAdd(&s_cnt[k], n_ok);
 #pragma unroll
       for (uint32_t a = 0; a < SJB_MAX_ATTRS; ++a) {
-        if (a < na) {
+        if (a < na && ((J.stats_mask >> a) & 1u)) {
           const uint32_t mx = __reduce_max_sync(kFull, ok ? uv[a] : 0u);
           const uint32_t mn = __reduce_max_sync(kFull, ok ? ~uv[a] : 0u);
           if (lane == 0) {
@@ -177,9 +181,11 @@ __global__ void __launch_bounds__(kBuildThreads) sjb_build_kernel(const __grid_c
   __syncthreads();
   for (uint32_t k = tid; k < nj; k += kBuildThreads) {
     if (!s_cnt[k]) continue;
+    const uint32_t mask = s_job[k].stats_mask;
     SjbEntryStats* st = s_job[k].stats;
-    atomicAdd(&st->count, s_cnt[k]);
+    if (!(mask & kJobStatsOnly)) atomicAdd(&st->count, s_cnt[k]);
     for (uint32_t a = 0; a < na; ++a) {
+      if (!((mask >> a) & 1u)) continue;
       atomicMax(&st->umax[a], s_umax[k][a]);
       atomicMax(&st->nmin[a], s_nmin[k][a]);
     }

@@ -143,6 +143,7 @@ sj_status schema_register(sj_engine* eng, const sjb_schema* sc, SchemaState& st)
       J.kind = SJ_PRED_ALL;
       J.words = st.words[d];
       J.in_index = -1;
+      J.stats_mask = kJobAllStats;  // the schema's attribute ranges
       J.bitmap = bm + wo;
       J.stats = stats + d;
       wo += st.words[d];
@@ -409,8 +410,41 @@ extern "C" sj_status sjb_batch_run(sjb_batch* b, const sjb_query* queries, int32
   std::unordered_map<std::string, int> local;  // dedupe within the batch when the cache is off
   uint32_t n_in = 0;
   uint64_t built = 0, cached = 0;
+  // a filter this batch created but did not build leaves the cache
   auto release_all = [&]() {
-    for (int id : held) b->cache.release(id);
+    for (int id : held)
+      if (b->cache.at(id).built) b->cache.release(id);
+      else b->cache.discard_new(id);
+  };
+  // Jobs this batch: a full build for each new filter, and a statistics-only job
+  // for a cached filter that lacks the min/max of an attribute some query here
+  // groups by.  job_of maps an entry to its job of this batch.
+  std::unordered_map<int, uint32_t> job_of;
+  std::vector<int> job_entry;
+  auto add_job = [&](int id, uint32_t mask) -> bool {
+    const FilterEntry& fe = b->cache.at(id);
+    if (fe.kind == SJ_PRED_IN && n_in >= (uint32_t)kBMaxIn) return false;
+    SjbJob& J = D.jobs[D.n_jobs];
+    memset(&J, 0, sizeof(J));
+    J.dim = fe.dim;
+    J.attr = fe.kind == SJ_PRED_ALL ? -1 : fe.attr;
+    J.kind = fe.kind;
+    J.lo = fe.lo;
+    J.hi = fe.hi;
+    J.words = b->S.words[fe.dim];
+    J.in_index = -1;
+    J.stats_mask = mask;
+    if (fe.kind == SJ_PRED_IN) {
+      J.in_index = (int32_t)n_in;
+      uint32_t* bits = D.in_bits[n_in++];
+      memset(bits, 0, sizeof(uint32_t) * kBInWords);
+      for (int32_t c : fe.codes) bits[c >> 5] |= 1u << (c & 31);
+    }
+    J.bitmap = b->cache.bitmap(id);
+    J.stats = b->cache.stats(id);
+    job_of[id] = D.n_jobs++;
+    job_entry.push_back(id);
+    return true;
   };
   for (int i = 0; i < n; ++i) {
     const sjb_query& q = queries[i];
@@ -421,6 +455,7 @@ extern "C" sj_status sjb_batch_run(sjb_batch* b, const sjb_query* queries, int32
     Q.n_preds = (uint32_t)q.n_preds;
     for (int k = 0; k < q.n_preds; ++k) {
       const sjb_pred& p = q.preds[k];
+      const uint32_t gbit = p.group_attr >= 0 ? 1u << p.group_attr : 0u;
       int id = -1;
       bool is_new = false;
       const std::string key = FilterCache::make_key(p, nullptr);
@@ -436,32 +471,21 @@ extern "C" sj_status sjb_batch_run(sjb_batch* b, const sjb_query* queries, int32
         }
         held.push_back(id);
         local[key] = id;
-        if (is_new) {
-          if (p.kind == SJ_PRED_IN && n_in >= (uint32_t)kBMaxIn) {
-            release_all();
-            return fail_fmt(SJ_ERR_UNSUPPORTED, "more than %d new IN-list filters in one batch", kBMaxIn);
-          }
-          SjbJob& J = D.jobs[D.n_jobs++];
-          memset(&J, 0, sizeof(J));
-          J.dim = (uint32_t)p.dim;
-          J.attr = p.kind == SJ_PRED_ALL ? -1 : p.attr;
-          J.kind = p.kind;
-          J.lo = p.lo;
-          J.hi = p.hi;
-          J.words = b->S.words[p.dim];
-          J.in_index = -1;
-          if (p.kind == SJ_PRED_IN) {
-            J.in_index = (int32_t)n_in;
-            uint32_t* bits = D.in_bits[n_in++];
-            memset(bits, 0, sizeof(uint32_t) * kBInWords);
-            for (int c = 0; c < p.in_count; ++c) bits[p.in_codes[c] >> 5] |= 1u << (p.in_codes[c] & 31);
-          }
-          J.bitmap = b->cache.bitmap(id);
-          J.stats = b->cache.stats(id);
-          ++built;
-        } else {
-          ++cached;
-        }
+        if (is_new) ++built;
+        else ++cached;
+      }
+      auto jt = job_of.find(id);
+      bool ok = true;
+      if (jt != job_of.end()) {
+        D.jobs[jt->second].stats_mask |= gbit;  // built or completed in this batch
+      } else if (is_new) {
+        ok = add_job(id, gbit);
+      } else if (gbit & ~b->cache.at(id).stats_have) {
+        ok = add_job(id, kJobStatsOnly | (gbit & ~b->cache.at(id).stats_have));
+      }
+      if (!ok) {
+        release_all();
+        return fail_fmt(SJ_ERR_UNSUPPORTED, "more than %d IN-list filters to build in one batch", kBMaxIn);
       }
       Q.dim[k] = (uint32_t)p.dim;
       Q.group_attr[k] = p.group_attr;
@@ -476,6 +500,7 @@ extern "C" sj_status sjb_batch_run(sjb_batch* b, const sjb_query* queries, int32
     return cuda_fail(e, "batch pipeline");
   }
   for (int id : held) b->cache.at(id).built = true;
+  for (uint32_t j = 0; j < D.n_jobs; ++j) b->cache.at(job_entry[j]).stats_have |= D.jobs[j].stats_mask & kJobAllStats;
   e = cudaGetLastError();  // an error no call above reported
   if (e != cudaSuccess) {
     release_all();

@@ -150,6 +150,7 @@ struct FilterEntry {
   bool live = false;
   SjbEntryStats host{};          // copy read back after the build (serving)
   bool host_valid = false;
+  uint32_t stats_have = 0;       // attributes whose min/max the statistics hold
 };
 
 class FilterCache {
@@ -234,6 +235,17 @@ class FilterCache {
     if (--e.refs > 0) return;
     auto it = index_.find(e.key);
     if (it == index_.end() || it->second != id) drop(id);
+  }
+
+  // Drop one reference to an entry acquire() just created and that will not be
+  // built (its job did not fit, or the call failed first): it leaves the index,
+  // so no later acquire finds an unbuilt filter.
+  void discard_new(int id) {
+    FilterEntry& e = entries_[id];
+    if (--e.refs > 0) return;
+    auto it = index_.find(e.key);
+    if (it != index_.end() && it->second == id) index_.erase(it);
+    drop(id);
   }
 
   void clear_unreferenced() {

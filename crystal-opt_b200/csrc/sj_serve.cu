@@ -215,7 +215,37 @@ bool admit(sjs_server* s) {
   D.n_jobs = 0;
   uint32_t n_in = 0;
   uint64_t hits = 0;
-  std::vector<int> new_ids;
+  std::vector<int> new_ids;  // entries built or completed this round (statistics read back)
+  // A full build for each new filter; a statistics-only job for a built filter
+  // that lacks the min/max of an attribute an admitted query groups by.
+  std::unordered_map<int, uint32_t> job_of;
+  std::vector<int> job_entry;
+  auto add_job = [&](int eid, uint32_t mask) -> bool {
+    const FilterEntry& fe = s->cache.at(eid);
+    if (D.n_jobs >= (uint32_t)kBMaxJobs || (fe.kind == SJ_PRED_IN && n_in >= (uint32_t)kBMaxIn)) return false;
+    SjbJob& J = D.jobs[D.n_jobs];
+    memset(&J, 0, sizeof(J));
+    J.dim = fe.dim;
+    J.attr = fe.kind == SJ_PRED_ALL ? -1 : fe.attr;
+    J.kind = fe.kind;
+    J.lo = fe.lo;
+    J.hi = fe.hi;
+    J.words = s->S.words[fe.dim];
+    J.in_index = -1;
+    J.stats_mask = mask;
+    if (fe.kind == SJ_PRED_IN) {
+      J.in_index = (int32_t)n_in;
+      uint32_t* bits = D.in_bits[n_in++];
+      memset(bits, 0, sizeof(uint32_t) * kBInWords);
+      for (int32_t c : fe.codes) bits[c >> 5] |= 1u << (c & 31);
+    }
+    J.bitmap = s->cache.bitmap(eid);
+    J.stats = s->cache.stats(eid);
+    job_of[eid] = D.n_jobs++;
+    job_entry.push_back(eid);
+    new_ids.push_back(eid);
+    return true;
+  };
   for (uint64_t id : cand) {
     Adm a{id, {-1, -1, -1, -1}, 0, {}};
     {
@@ -236,37 +266,30 @@ bool admit(sjs_server* s) {
     bool ok = true;
     for (int k = 0; k < tq.n_preds && ok; ++k) {
       const sjb_pred& p = tq.preds[k];
+      const uint32_t gbit = p.group_attr >= 0 ? 1u << p.group_attr : 0u;
       bool is_new = false;
       const int eid = s->cache.acquire(p, s->S.words[p.dim], s->cfg.limits.cache_filters != 0, &is_new);
-      if (eid < 0 || (is_new && (D.n_jobs >= (uint32_t)kBMaxJobs ||
-                                 (p.kind == SJ_PRED_IN && n_in >= (uint32_t)kBMaxIn)))) {
-        if (eid >= 0) s->cache.release(eid);
+      if (eid < 0) {
+        ok = false;
+        break;
+      }
+      auto jt = job_of.find(eid);
+      bool fits = true;
+      if (jt != job_of.end()) {
+        D.jobs[jt->second].stats_mask |= gbit;  // built or completed this round
+      } else if (is_new) {
+        fits = add_job(eid, gbit);
+      } else if (gbit & ~s->cache.at(eid).stats_have) {
+        fits = add_job(eid, kJobStatsOnly | (gbit & ~s->cache.at(eid).stats_have));
+      }
+      if (!fits) {
+        if (is_new) s->cache.discard_new(eid);
+        else s->cache.release(eid);
         ok = false;
         break;
       }
       a.entry[a.n++] = eid;
-      if (is_new) {
-        SjbJob& J = D.jobs[D.n_jobs++];
-        memset(&J, 0, sizeof(J));
-        J.dim = (uint32_t)p.dim;
-        J.attr = p.kind == SJ_PRED_ALL ? -1 : p.attr;
-        J.kind = p.kind;
-        J.lo = p.lo;
-        J.hi = p.hi;
-        J.words = s->S.words[p.dim];
-        J.in_index = -1;
-        if (p.kind == SJ_PRED_IN) {
-          J.in_index = (int32_t)n_in;
-          uint32_t* bits = D.in_bits[n_in++];
-          memset(bits, 0, sizeof(uint32_t) * kBInWords);
-          for (int c = 0; c < p.in_count; ++c) bits[p.in_codes[c] >> 5] |= 1u << (p.in_codes[c] & 31);
-        }
-        J.bitmap = s->cache.bitmap(eid);
-        J.stats = s->cache.stats(eid);
-        new_ids.push_back(eid);
-      } else {
-        ++hits;
-      }
+      if (!is_new) ++hits;
     }
     if (!ok) {
       for (int k = 0; k < a.n; ++k) s->cache.release(a.entry[k]);
@@ -306,8 +329,13 @@ bool admit(sjs_server* s) {
       e.host_valid = true;
       e.built = true;
     }
+    uint64_t full_builds = 0;
+    for (uint32_t j = 0; j < D.n_jobs; ++j) {
+      s->cache.at(job_entry[j]).stats_have |= D.jobs[j].stats_mask & kJobAllStats;
+      full_builds += (D.jobs[j].stats_mask & kJobStatsOnly) ? 0u : 1u;
+    }
     std::lock_guard<std::mutex> g(s->mu);
-    s->stats.filters_built += new_ids.size();
+    s->stats.filters_built += full_builds;
   }
   // group layout and accumulator ranges
   const double t_adm = now_s();

@@ -72,10 +72,16 @@ struct SjbJob {
   int32_t lo, hi;
   uint32_t words;        // bitmap words (ceil(len / 32))
   int32_t in_index;      // row of the IN-code bitmaps, -1 if none
-  uint32_t pad;
+  uint32_t stats_mask;   // bit a: reduce min/max of attribute a; kJobStatsOnly: see below
   uint32_t* bitmap;
   SjbEntryStats* stats;
 };
+
+// A job that only adds attributes' min/max to the statistics of a filter that is
+// already built (and may be in use): it neither zeroes nor writes the bitmap and
+// leaves the count alone.
+constexpr uint32_t kJobStatsOnly = 1u << 31;
+constexpr uint32_t kJobAllStats = (1u << SJB_MAX_ATTRS) - 1u;
 
 struct SjbAcc {
   unsigned long long cnt;

@@ -285,8 +285,31 @@ static void test_bf_effective() {
       if (bf_effective(kBfAuto, lg, 16, ins, 0, &l2) == kBfBlocked) CHECK((8ull << l2) < (1ull << lg) / 8);
 }
 
+// A filter created by acquire() but never built leaves the index when it is
+// discarded: the next acquire of the same predicate builds it anew.
+static void test_filter_cache_discard() {
+  std::vector<uint8_t> arena(256 * 4);
+  std::vector<SjbEntryStats> stats(4);
+  FilterCache c;
+  c.init(arena.data(), arena.size(), stats.data(), 4);
+  bool is_new = false;
+  const int a = c.acquire(range_pred(0, 1, 5), 64, true, &is_new);
+  CHECK(a >= 0 && is_new);
+  c.discard_new(a);
+  const int b = c.acquire(range_pred(0, 1, 5), 64, true, &is_new);
+  CHECK(b >= 0 && is_new);  // not served from the cache
+  c.at(b).built = true;
+  c.release(b);
+  const int b2 = c.acquire(range_pred(0, 1, 5), 64, true, &is_new);
+  CHECK(b2 == b && !is_new);  // a built, released filter is cached
+  // the discarded entry's arena range and id were freed: three more fit
+  c.release(b2);
+  for (int k = 1; k <= 3; ++k) CHECK(c.acquire(range_pred(k, 0, 0), 64, true, &is_new) >= 0 && is_new);
+}
+
 int main() {
   test_bf_effective();
+  test_filter_cache_discard();
   test_perms();
   test_range_alloc();
   test_filter_cache();

@@ -155,3 +155,27 @@ def test_colliding_dimension_keys_are_refused(sj, engine, star, torch_cuda):
     with pytest.raises(sj.StarJoinError) as e:
         ss.Batch(engine, sc, cols)
     assert e.value.status == sj.SJ_ERR_UNSUPPORTED
+
+
+def test_cached_filter_regrouped(oracle, engine, star):
+    """A cached filter carries the min/max of the attributes its queries grouped
+    by; a later batch that reuses it grouped by another attribute completes its
+    statistics (a statistics-only build job, the bitmap untouched) and still
+    answers like the oracle -- in the same batch and across batches."""
+    sc, host, dev = star
+    b = ss.Batch(engine, sc, dev, use_graph=True, cache_filters=True)
+    try:
+        def q(group_attr, other_group):
+            return {"preds": [{"dim": 0, "kind": "range", "attr": 1, "lo": 100, "hi": 700, "group_attr": group_attr},
+                              {"dim": 1, "kind": "range", "attr": 1, "lo": 0, "hi": 300, "group_attr": other_group}],
+                    "row_range": (0, sc.fact_rows)}
+        first = [q(0, -1)]                 # supplier filter, statistics of attribute 0
+        later = [q(1, -1), q(2, 0)]        # the same filters grouped by attributes 1 and 2
+        mixed = [q(0, 1), q(1, 2), q(-1, 0)]
+        for batch_qs in (first, later, mixed):
+            got = b.run(batch_qs)
+            for g, bq in zip(got, batch_qs):
+                assert g == oracle.run(ss.to_plain(sc, bq), host)
+        assert b.stats().filters_cached > 0
+    finally:
+        b.close()

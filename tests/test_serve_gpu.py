@@ -248,3 +248,25 @@ def test_solo_plain_cancelled_ticket(sj, engine, star):
         assert sum(r[-2] for r in rows) == 5000
     finally:
         srv.close()
+
+
+def test_cached_filter_regrouped_while_serving(oracle, engine, star):
+    """Serving: a query that reuses a cached filter grouped by an attribute the
+    filter has no statistics for gets them completed at admission; every answer
+    equals the oracle's."""
+    sc, host, dev = star
+    srv = ss.Server(engine, sc, dev, cache_filters=True, step_rows=1 << 20)
+    try:
+        def q(g0, g1):
+            return {"preds": [{"dim": 0, "kind": "range", "attr": 1, "lo": 50, "hi": 650, "group_attr": g0},
+                              {"dim": 1, "kind": "range", "attr": 1, "lo": 100, "hi": 900, "group_attr": g1}],
+                    "row_range": (0, sc.fact_rows)}
+        for g0, g1 in ((0, -1), (1, 0), (2, 1), (-1, 2)):
+            qq = q(g0, g1)
+            rows, info = srv.wait(srv.submit(qq), timeout_s=120.0)
+            assert info.status == 0
+            assert rows == oracle.run(ss.to_plain(sc, qq), host)
+        st = srv.stats()
+        assert st.filters_built == 2 and st.filters_cached >= 6
+    finally:
+        srv.close()
