@@ -171,7 +171,7 @@ def test_cached_filter_regrouped(oracle, engine, star):
                     "row_range": (0, sc.fact_rows)}
         first = [q(0, -1)]                 # supplier filter, statistics of attribute 0
         later = [q(1, -1), q(2, 0)]        # the same filters grouped by attributes 1 and 2
-        mixed = [q(0, 1), q(1, 2), q(-1, 0)]
+        mixed = [q(0, 1), q(2, 1), q(-1, 2)]  # group spans within the batch's 16M accumulators
         for batch_qs in (first, later, mixed):
             got = b.run(batch_qs)
             for g, bq in zip(got, batch_qs):

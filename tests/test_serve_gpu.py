@@ -261,9 +261,10 @@ def test_cached_filter_regrouped_while_serving(oracle, engine, star):
             return {"preds": [{"dim": 0, "kind": "range", "attr": 1, "lo": 50, "hi": 650, "group_attr": g0},
                               {"dim": 1, "kind": "range", "attr": 1, "lo": 100, "hi": 900, "group_attr": g1}],
                     "row_range": (0, sc.fact_rows)}
-        for g0, g1 in ((0, -1), (1, 0), (2, 1), (-1, 2)):
+        # each query's worst group span (full attribute ranges) within the server's 1M result rows
+        for g0, g1 in ((0, -1), (1, 0), (2, 0), (-1, 2)):
             qq = q(g0, g1)
-            rows, info = srv.wait(srv.submit(qq), timeout_s=120.0)
+            rows, info = srv.wait(srv.submit(qq), timeout_s=120.0, cap=1 << 20)
             assert info.status == 0
             assert rows == oracle.run(ss.to_plain(sc, qq), host)
         st = srv.stats()
