@@ -868,18 +868,25 @@ extern "C" sj_status sj_bloom_test(const int32_t* keys, const int32_t* flags, in
 }
 
 // ------------------------------------------------------------ generators ----
-__global__ void sj_gen_kernel(int32_t* dst, int64_t n, uint64_t key, int32_t kind, int32_t lo, int32_t hi) {
+__global__ void sj_gen_kernel(int32_t* dst, int64_t n, uint64_t row0, uint64_t key, int32_t kind, int32_t lo,
+                              int32_t hi) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    dst[i] = sj_gen_value(key, kind, lo, hi, (uint64_t)i);
+    dst[i] = sj_gen_value(key, kind, lo, hi, row0 + (uint64_t)i);
+}
+
+extern "C" sj_status sj_gen_rows_device(int32_t* dst, int64_t row0, int64_t n, uint64_t seed, int32_t col,
+                                        int32_t kind, int32_t lo, int32_t hi, void* stream) {
+  if (n < 0 || row0 < 0 || (n && !dst)) return fail(SJ_ERR_INVALID_ARGUMENT, "bad buffer");
+  if (n == 0) return SJ_OK;
+  sj_gen_kernel<<<1184, 256, 0, (cudaStream_t)stream>>>(dst, n, (uint64_t)row0, sj_stream_key(seed, (uint32_t)col),
+                                                        kind, lo, hi);
+  SJ_CUDA(cudaGetLastError());
+  return SJ_OK;
 }
 
 extern "C" sj_status sj_gen_column_device(int32_t* dst, int64_t n, uint64_t seed, int32_t col, int32_t kind,
                                           int32_t lo, int32_t hi, void* stream) {
-  if (n < 0 || (n && !dst)) return fail(SJ_ERR_INVALID_ARGUMENT, "bad buffer");
-  if (n == 0) return SJ_OK;
-  sj_gen_kernel<<<1184, 256, 0, (cudaStream_t)stream>>>(dst, n, sj_stream_key(seed, (uint32_t)col), kind, lo, hi);
-  SJ_CUDA(cudaGetLastError());
-  return SJ_OK;
+  return sj_gen_rows_device(dst, 0, n, seed, col, kind, lo, hi, stream);
 }
 
 // Host generator (no GPU needed): same values as sj_gen_column_device.

@@ -21,7 +21,6 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "sj_internal.h"
@@ -54,25 +53,19 @@ static sj_status na_fail(sj_status s, const char* fmt, ...) {
   return s;
 }
 
-// Device address of the scratch array, looked up once per device with that
-// device current (the host-side symbol itself is not a device address).
+// Device address of the scratch array in the current device's context (the
+// host-side symbol itself is not a device address).  Looked up on every call,
+// with the call's device current: the lookup allocates nothing, and an address
+// cached across calls would go stale when the caller resets the device
+// (cudaDeviceReset) and the library's device code is loaded into a new context.
 static sj_status scratch_address(int device, unsigned char** out) {
-  static std::mutex mu;
-  static unsigned char* addr[64] = {};
-  static bool have[64] = {};
-  if (device < 0 || device >= 64) return na_fail(SJ_ERR_INVALID_ARGUMENT, "device %d out of range", device);
-  std::lock_guard<std::mutex> lock(mu);
-  if (!have[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, sj_noalloc_scratch);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return na_fail(SJ_ERR_CUDA, "cudaGetSymbolAddress(scratch) on device %d: %s", device, cudaGetErrorString(e));
-    }
-    addr[device] = static_cast<unsigned char*>(p);
-    have[device] = true;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, sj_noalloc_scratch);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return na_fail(SJ_ERR_CUDA, "cudaGetSymbolAddress(scratch) on device %d: %s", device, cudaGetErrorString(e));
   }
-  *out = addr[device];
+  *out = static_cast<unsigned char*>(p);
   return SJ_OK;
 }
 
@@ -156,8 +149,9 @@ extern "C" sj_status sj_ssb_q33_run_noalloc(int device, const int32_t* lo_orderd
   unsigned char* base = nullptr;
   sj_status s = scratch_address(device, &base);
   if (s != SJ_OK) return s;
-  int sms = 0;
+  int sms = 0, smem_optin = 0;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   if (e != cudaSuccess) return na_fail(SJ_ERR_CUDA, "device attribute: %s", cudaGetErrorString(e));
 
   // ---- runtime parameters
@@ -220,10 +214,13 @@ extern "C" sj_status sj_ssb_q33_run_noalloc(int device, const int32_t* lo_orderd
   rt.bf_smem_budget = g.bf_smem_bytes;
   g.group_smem_cap = 1024;
   g.q1_cap = 512;
-  g.q2_cap = 64;
+  g.q2_cap = 128;  // room for a two-survivors-per-lane Q1 round (64) over a partial Q2
   g.reorder_period = 16;
   g.grid = (uint32_t)sms;
   g.smem_bytes = probe_smem_bytes(g);
+  if (g.smem_bytes > (uint32_t)smem_optin)
+    return na_fail(SJ_ERR_UNSUPPORTED, "probe needs %u bytes of shared memory per block; device %d allows %d",
+                   g.smem_bytes, device, smem_optin);
 
   // ---- clear, upload the IN lists, build, probe, finalize, read back
   auto check = [&](cudaError_t ce, const char* what) -> sj_status {
@@ -251,7 +248,9 @@ extern "C" sj_status sj_ssb_q33_run_noalloc(int device, const int32_t* lo_orderd
     return s;
   if ((s = check(cudaStreamSynchronize(st), "synchronize")) != SJ_OK) return s;
   if (desc.error_flags & kErrWaitTimeout) return na_fail(SJ_ERR_TIMEOUT, "probe kernel: bounded wait expired");
-  if (desc.error_flags) return na_fail(SJ_ERR_INVALID_ARGUMENT, "device error flags 0x%x", desc.error_flags);
+  if (desc.error_flags & kErrPayloadDomain)
+    return na_fail(SJ_ERR_INVALID_ARGUMENT, "a grouped payload lies outside [payload_min, payload_max]");
+  if (desc.error_flags) return na_fail(SJ_ERR_CUDA, "device error flags 0x%x", desc.error_flags);
   *n_out = desc.groups_out;
   if ((int64_t)desc.groups_out > cap || (desc.groups_out && !out))
     return na_fail(SJ_ERR_CAPACITY, "need %u result rows", desc.groups_out);

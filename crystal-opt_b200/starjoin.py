@@ -142,6 +142,8 @@ def load(build_if_missing: bool = True) -> C.CDLL:
                                     C.c_int32, P]),
         "sj_gen_column_device": (C.c_int, [P, C.c_int64, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
                                            C.c_int32, P]),
+        "sj_gen_rows_device": (C.c_int, [P, C.c_int64, C.c_int64, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
+                                         C.c_int32, P]),
         "sj_gen_column_host": (None, [P, C.c_int64, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
                                       C.c_int32, C.c_int]),
         "sj_ssb_q33_run_noalloc": (C.c_int, [C.c_int] + [P] * 4 + [C.c_int64] + [P] * 2 + [C.c_int64] +
@@ -168,7 +170,7 @@ def exported_symbols() -> List[str]:
         "sj_engine_create", "sj_engine_destroy", "sj_status_string", "sj_last_error",
         "sj_device_sm_count", "sj_query_prepare", "sj_query_build", "sj_query_probe",
         "sj_query_fetch", "sj_query_get_stats", "sj_query_release", "sj_run_plain",
-        "sj_ssb_q33_run", "sj_bloom_test", "sj_gen_column_device", "sj_gen_column_host",
+        "sj_ssb_q33_run", "sj_bloom_test", "sj_gen_column_device", "sj_gen_rows_device", "sj_gen_column_host",
         "sj_ssb_q33_run_noalloc", "sj_noalloc_last_error", "sj_autotune",
         "sj_ssb_column_file", "sj_ssb_load_column", "sj_ssb_store_column",
     ]
@@ -261,8 +263,11 @@ def gen_host(schema: StarSchema, names: Optional[Sequence[str]] = None, threads:
     return {k: v for k, v in out.items() if k in want}
 
 
-def gen_device(schema: StarSchema, names: Optional[Sequence[str]] = None, device: int = 0):
-    """Generate columns directly into torch CUDA tensors (same values as gen_host)."""
+def gen_device(schema: StarSchema, names: Optional[Sequence[str]] = None, device: int = 0,
+               fact_range: Optional[Sequence[int]] = None):
+    """Generate columns directly into torch CUDA tensors (same values as gen_host).
+    fact_range=(b, e): only rows [b, e) of the fact columns (one shard of the
+    schema's fact table); dimension columns are always whole."""
     import torch
     lib = load()
     bases, derived, want = _wanted(schema, names)
@@ -270,8 +275,11 @@ def gen_device(schema: StarSchema, names: Optional[Sequence[str]] = None, device
     for name, (n, col, kind, lo, hi) in schema.column_specs().items():
         if name not in bases:
             continue
+        row0 = 0
+        if fact_range is not None and n == schema.fact_rows:
+            row0, n = int(fact_range[0]), int(fact_range[1]) - int(fact_range[0])
         t = torch.empty(max(n, 1), dtype=torch.int32, device=f"cuda:{device}")[:n]
-        check(lib.sj_gen_column_device(t.data_ptr(), n, schema.seed, col, kind, lo, hi, None))
+        check(lib.sj_gen_rows_device(t.data_ptr(), row0, n, schema.seed, col, kind, lo, hi, None))
         out[name] = t
     for name in derived:
         base, div = schema.derived_specs()[name]

@@ -205,9 +205,11 @@ sj_status sj_ssb_q33_run(sj_engine* e,
  * 48 MiB file-scope device array that every GPU loading this library holds until
  * the process exits; queries needing more return SJ_ERR_CAPACITY (dimension
  * tables up to about 1.2M customer + supplier rows fit).  Column pointers are
- * device memory; `out` is a host buffer of `cap` rows.  The first call on a
- * device looks up the array's device address (make it before any stream
- * capture).  Calls share the array and keep the last call's contents (each call
+ * device memory; `out` is a host buffer of `cap` rows.  Every call looks up
+ * the array's device address with `device` current (the lookup allocates
+ * nothing and stays valid across cudaDeviceReset); the first call on a device
+ * also loads the library's device code there, so make it before any stream
+ * capture.  Calls share the array and keep the last call's contents (each call
  * clears what must start at zero); calls that overlap on the GPU race, so
  * serialize them.  Errors: sj_noalloc_last_error(). */
 sj_status sj_ssb_q33_run_noalloc(int device,
@@ -280,6 +282,10 @@ sj_status sj_ssb_store_column(const char* dir, const char* column, int64_t n, co
 /* Fill dst[0..n) with generated column values (see sj_datagen.h kinds). */
 sj_status sj_gen_column_device(int32_t* dst, int64_t n, uint64_t seed, int32_t col,
                                int32_t kind, int32_t lo, int32_t hi, void* stream);
+/* Rows [row0, row0 + n) of the same column into dst[0..n): one shard of a table
+ * that several GPUs split by rows, each generating only its own part. */
+sj_status sj_gen_rows_device(int32_t* dst, int64_t row0, int64_t n, uint64_t seed, int32_t col,
+                             int32_t kind, int32_t lo, int32_t hi, void* stream);
 /* Host form of the same generator (needs no GPU); threads <= 0 uses all cores. */
 void sj_gen_column_host(int32_t* dst, int64_t n, uint64_t seed, int32_t col,
                         int32_t kind, int32_t lo, int32_t hi, int threads);

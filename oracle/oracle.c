@@ -177,3 +177,49 @@ done:
   free(base.cnt);
   return rc;
 }
+
+/* ---- seeded synthetic columns (the generator header is plain C) ---------- */
+#include "../crystal-opt_b200/csrc/sj_datagen.h"
+
+typedef struct or_gen_job {
+  int32_t* dst;
+  int64_t begin, end, row0;
+  uint64_t key;
+  int32_t kind, lo, hi;
+} or_gen_job;
+
+static void* or_gen_worker(void* arg) {
+  const or_gen_job* j = (const or_gen_job*)arg;
+  for (int64_t i = j->begin; i < j->end; ++i)
+    j->dst[i] = sj_gen_value(j->key, j->kind, j->lo, j->hi, (uint64_t)(j->row0 + i));
+  return NULL;
+}
+
+void or_gen_column(int32_t* dst, int64_t n, uint64_t seed, int32_t col, int32_t kind, int32_t lo, int32_t hi,
+                   int threads) {
+  or_gen_rows(dst, 0, n, seed, col, kind, lo, hi, threads);
+}
+
+void or_gen_rows(int32_t* dst, int64_t row0, int64_t n, uint64_t seed, int32_t col, int32_t kind, int32_t lo,
+                 int32_t hi, int threads) {
+  if (n <= 0 || row0 < 0) return;
+  if (threads <= 0) threads = or_available_cores();
+  if (threads > 256) threads = 256;
+  if (n < (int64_t)threads * 65536) threads = (int)(n / 65536) + 1;
+  or_gen_job jobs[256];
+  pthread_t tids[256];
+  const uint64_t key = sj_stream_key(seed, (uint32_t)col);
+  for (int t = 0; t < threads; ++t) {
+    jobs[t].dst = dst;
+    jobs[t].begin = n * t / threads;
+    jobs[t].end = n * (t + 1) / threads;
+    jobs[t].row0 = row0;
+    jobs[t].key = key;
+    jobs[t].kind = kind;
+    jobs[t].lo = lo;
+    jobs[t].hi = hi;
+  }
+  for (int t = 1; t < threads; ++t) pthread_create(&tids[t], NULL, or_gen_worker, &jobs[t]);
+  or_gen_worker(&jobs[0]);
+  for (int t = 1; t < threads; ++t) pthread_join(tids[t], NULL);
+}

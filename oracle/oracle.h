@@ -75,6 +75,16 @@ int or_build_pht(const or_dim* d, int32_t* ht);
 /* Cores the process may run on. */
 int or_available_cores(void);
 
+/* Column `col` of the seeded synthetic schema (crystal-opt_b200/csrc/sj_datagen.h:
+ * SplitMix64 stream per column, value a pure function of (seed, col, row)) into
+ * dst[0, n), on `threads` host threads (<= 0: all cores).  Lets the benchmark's
+ * CPU legs generate their inputs without loading the engine's library. */
+void or_gen_column(int32_t* dst, int64_t n, uint64_t seed, int32_t col, int32_t kind, int32_t lo, int32_t hi,
+                   int threads);
+/* Rows [row0, row0 + n) of the same column into dst[0, n). */
+void or_gen_rows(int32_t* dst, int64_t row0, int64_t n, uint64_t seed, int32_t col, int32_t kind, int32_t lo,
+                 int32_t hi, int threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,9 +23,9 @@ MAX_DIMS = 4
 
 def build(force: bool = False) -> str:
     src = os.path.join(HERE, "oracle.c")
-    hdr = os.path.join(HERE, "oracle.h")
-    if (not force and os.path.exists(LIB)
-            and os.path.getmtime(LIB) >= max(os.path.getmtime(src), os.path.getmtime(hdr))):
+    deps = [src, os.path.join(HERE, "oracle.h"),
+            os.path.join(os.path.dirname(HERE), "crystal-opt_b200", "csrc", "sj_datagen.h")]
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     tmp = LIB + ".tmp"
@@ -68,12 +68,42 @@ def load() -> C.CDLL:
         lib.or_build_pht.restype = C.c_int
         lib.or_build_pht.argtypes = [C.POINTER(OrDim), C.c_void_p]
         lib.or_available_cores.restype = C.c_int
+        lib.or_gen_column.restype = None
+        lib.or_gen_column.argtypes = [C.c_void_p, C.c_int64, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
+                                      C.c_int32, C.c_int]
+        lib.or_gen_rows.restype = None
+        lib.or_gen_rows.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
+                                    C.c_int32, C.c_int]
         _lib = lib
     return _lib
 
 
 def cores() -> int:
     return int(load().or_available_cores())
+
+
+def gen_host(schema, names=None, threads: int = 0, fact_range=None) -> Dict[str, np.ndarray]:
+    """The schema's seeded columns generated by this library (same values as the
+    engine's generator), for CPU legs that must not load the engine.  `schema`
+    is a starjoin.StarSchema (its column specs are plain Python).
+    fact_range=(b, e): only rows [b, e) of the fact columns."""
+    lib = load()
+    derived_specs = schema.derived_specs()
+    want = set(schema.column_names()) if names is None else set(names)
+    bases = {n for n in want if n in schema.column_specs()} | {derived_specs[n][0] for n in want if n in derived_specs}
+    out: Dict[str, np.ndarray] = {}
+    for name, (n, col, kind, lo, hi) in schema.column_specs().items():
+        if name in bases:
+            row0 = 0
+            if fact_range is not None and n == schema.fact_rows:
+                row0, n = int(fact_range[0]), int(fact_range[1]) - int(fact_range[0])
+            a = np.empty(max(n, 0), dtype=np.int32)
+            lib.or_gen_rows(a.ctypes.data, row0, n, schema.seed, col, kind, lo, hi, threads)
+            out[name] = a
+    for name, (base, div) in derived_specs.items():
+        if name in want:
+            out[name] = (out[base] // div).astype(np.int32)
+    return {k: v for k, v in out.items() if k in want}
 
 
 def _plan(query: Dict[str, Any], cols: Dict[str, np.ndarray]):

@@ -3,7 +3,7 @@ Q2.1-Q2.3, Q3.1, Q3.2, Q3.4 and Q4.1-Q4.3) against this repository's
 crystal/*.cuh device functions (the drop-in check).
 
 Each driver (src/ssb-jo/q33/<order>-<lip|naive>.cu, compiled where it lies in
-the reference tree, default /root/reference or $CRYSTAL_OPT_REF) includes
+the reference tree that oracle/build_ref.py locates) includes
 "crystal/crystal.cuh"; with crystal-opt_b200/ first on the include path that
 resolves to the sm_100a reimplementation here, while the driver source itself
 stays unmodified.  The main() comes from oracle/ref_runner.cu (seeded synthetic
@@ -20,7 +20,6 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 OUT = os.path.join(HERE, "_dropin")
-REF = os.environ.get("CRYSTAL_OPT_REF", "/root/reference")
 
 
 def binary(order: int, method: str) -> str:
@@ -51,7 +50,7 @@ def _compile(order: int, method: str) -> str:
 
 
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
-from build_ref import SHAPE_SOURCES  # noqa: E402  (driver file of each other query)
+from build_ref import REF, SHAPE_SOURCES  # noqa: E402  (reference tree; driver file of each other query)
 
 SHAPES = tuple(SHAPE_SOURCES)
 
@@ -81,15 +80,37 @@ def _compile_shape(query: int) -> str:
     return out
 
 
+BLOCKSUM = os.path.join(OUT, "blocksum_test")
+
+
+def build_blocksum() -> str:
+    """tests/cpp/blocksum_test.cu (the drop-in BlockSum on the GPU against host
+    sums); needs no reference tree."""
+    src = os.path.join(HERE, "cpp", "blocksum_test.cu")
+    hdrs = [os.path.join(ROOT, "crystal-opt_b200", "crystal", f) for f in os.listdir(
+        os.path.join(ROOT, "crystal-opt_b200", "crystal"))]
+    if os.path.exists(BLOCKSUM) and os.path.getmtime(BLOCKSUM) >= max(os.path.getmtime(d) for d in [src] + hdrs):
+        return BLOCKSUM
+    os.makedirs(OUT, exist_ok=True)
+    cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+           "-I", os.path.join(ROOT, "crystal-opt_b200"), "-o", BLOCKSUM + ".tmp", src]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"{src}: {r.stderr[-2000:]}")
+    os.replace(BLOCKSUM + ".tmp", BLOCKSUM)
+    return BLOCKSUM
+
+
 def build(jobs: int = 0) -> list[str]:
+    built = [build_blocksum()]
     if not available():
-        return []
+        return built
     os.makedirs(OUT, exist_ok=True)
     jobs = jobs or min(8, os.cpu_count() or 1)
     with cf.ThreadPoolExecutor(jobs) as ex:
         futs = [ex.submit(_compile, o, m) for o in range(6) for m in ("lip", "naive")]
         futs += [ex.submit(_compile_shape, q) for q in SHAPES]
-        return [f.result() for f in futs]
+        return built + [f.result() for f in futs]
 
 
 if __name__ == "__main__":

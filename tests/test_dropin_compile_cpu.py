@@ -6,9 +6,9 @@ import concurrent.futures as cf
 
 import pytest
 
+from build_ref import REF  # the reference tree the build recipe reads
 from conftest import ROOT
 
-REF = os.environ.get("CRYSTAL_OPT_REF", "/root/reference")
 DRIVERS = ["src/ssb-jo/q21/0-lip.cu", "src/ssb-jo/q31/0-lip.cu", "src/ssb-jo/q32/3-naive.cu",
            "src/ssb-jo/q34/5-lip.cu", "src/ssb-jo/q41/0-lip.cu", "src/ops/bloom_join.cu", "src/ops/join.cu"]
 

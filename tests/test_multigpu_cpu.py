@@ -40,8 +40,8 @@ def _rank_main(rank, world, port, queries, out):
             b, e = multigpu.row_range(sc.fact_rows, rank, world)
             q["row_range"] = (b, e)
             part = oracle.run(q, cols, threads=2)
-            merged = multigpu.merge_groups(part, 3, dist)
-            results.append(merged)
+            results.append(multigpu.merge_groups(part, q, dist))
+            results.append(multigpu.merge_gather(part, 3, dist))
         out[rank] = results
     finally:
         dist.destroy_process_group()
@@ -70,7 +70,23 @@ def test_two_gloo_ranks_merge_to_the_single_run(sj, oracle, world):
     for i, cities in enumerate(queries):
         want = oracle.run(sj.q33_query(sc, cities=cities), cols)
         for r in range(world):
-            assert out[r][i] == want
+            assert out[r][2 * i] == want  # dense all-reduce
+            assert out[r][2 * i + 1] == want  # all-gather fallback
+
+
+def test_dense_merge_wraps_sums_modulo_2_64():
+    """Sums near 2^64 from several ranks add modulo 2^64 (two's-complement
+    uint64, as the engine's partials), through the 32-bit-halves layout."""
+    import multigpu
+
+    class FakeDist:  # all_reduce over three pretend ranks holding the same partials
+        def all_reduce(self, t):
+            t.mul_(3)
+
+    spans = [(1992, 7)]
+    rows = [(1995, 5, (1 << 64) - 7)]
+    got = multigpu.merge_dense(rows, spans, FakeDist())
+    assert got == [(1995, 15, (3 * ((1 << 64) - 7)) % (1 << 64))]
 
 
 def _dying_rank(rank, world, port, out):
@@ -85,7 +101,7 @@ def _dying_rank(rank, world, port, out):
         os._exit(3)  # the worker dies between steps, before the exchange
     t0 = time.time()
     try:
-        multigpu.merge_groups([(1, 2, 3, 4, 5)], 3, dist)
+        multigpu.merge_dense([(1, 2, 1993, 4, 5)], [(0, 250), (0, 250), (1992, 7)], dist)
         out[rank] = ("merged", time.time() - t0)
     except Exception as e:  # noqa: BLE001
         out[rank] = ("error", time.time() - t0, type(e).__name__)

@@ -140,3 +140,19 @@ def test_oracle_matches_reference_shape_golden(sj, oracle):
         assert want, q
         got = shape_as_printed(q, oracle.run(make(sc), cols))
         assert got == [tuple(w) for w in want], q
+
+
+def test_oracle_generator_matches_engine_generator(sj):
+    """The oracle library's copy of the seeded generator (used by the benchmark's
+    reference arm, which must not load the engine) gives the engine's columns."""
+    import oracle
+    sc = sj.StarSchema(seed=424242, fact_rows=200_003, cust_rows=3001, supp_rows=401, part_rows=1501)
+    a, b = oracle.gen_host(sc), sj.gen_host(sc)
+    assert a.keys() == b.keys()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    lo, hi = 70_001, 150_013  # one shard of the fact rows
+    shard = oracle.gen_host(sc, ["fk_cust", "revenue", "c_city"], fact_range=(lo, hi))
+    assert np.array_equal(shard["fk_cust"], a["fk_cust"][lo:hi])
+    assert np.array_equal(shard["revenue"], a["revenue"][lo:hi])
+    assert np.array_equal(shard["c_city"], a["c_city"])
