@@ -154,8 +154,9 @@ def _poisson_run(srv: ss.Server, queries: List[Dict[str, Any]], rate: float, see
     }, rows
 
 
-def serving(eng: sj.Engine, rates=(200.0, 2000.0), seconds: float = 1.0, seed: int = 77,
-            schema: Dict[str, int] = None, plain_cap: int = 300, flood: int = 256, threads: int = 0) -> Dict[str, Any]:
+def serving(eng: sj.Engine, rates=(50.0, 200.0, 2000.0), seconds: float = 1.0, seed: int = 77,
+            schema: Dict[str, int] = None, plain_cap: int = 300, flood: int = 2048, mixes: int = 3,
+            threads: int = 0) -> Dict[str, Any]:
     sc = sj.StarSchema(**(schema or SERVE_SCHEMA))
     dev = sj.gen_device(sc)
     rng = random.Random(seed)
@@ -196,25 +197,34 @@ def serving(eng: sj.Engine, rates=(200.0, 2000.0), seconds: float = 1.0, seed: i
             srv.close()
         exact = exact and plain_rows == shared_rows[:m]
         out["rates"].append({"shared": shared, "shared_solo_plain": solo, "plain": plain})
-    # saturation: every query submitted at once -- the loops' capacity
+    # saturation: every query of a mix submitted at once -- the loops' capacity,
+    # over several seeded mixes of `flood` queries each
     if flood:
-        qs = [ss.random_query(rng, sc) for _ in range(flood)]
-        res = {}
-        for plain in (False, True):
-            srv = ss.Server(eng, sc, dev, plain=plain, cache_filters=True, threads=threads)
-            try:
-                r, rows = _poisson_run(srv, qs, float("inf"), seed)
-                st = srv.stats()
-                r.update({"steps": st.steps, "busy_s": st.busy_s, "admit_s": st.admit_s, "scan_s": st.scan_s,
-                          "probe_device_s": st.probe_device_s, "peak_active": st.peak_active,
-                          "rows_scanned": st.rows_scanned})
-            finally:
-                srv.close()
-            res["plain" if plain else "shared"] = r
-            res["rows_plain" if plain else "rows_shared"] = rows
-        exact = exact and res.pop("rows_plain") == res.pop("rows_shared")
-        res["speedup_vs_plain"] = res["shared"]["throughput_qps"] / max(res["plain"]["throughput_qps"], 1e-9)
-        out["saturation"] = res
+        runs = []
+        for mix in range(mixes):
+            mrng = random.Random(seed * 1009 + mix)
+            qs = [ss.random_query(mrng, sc) for _ in range(flood)]
+            res = {"seed": seed * 1009 + mix}
+            for plain in (False, True):
+                srv = ss.Server(eng, sc, dev, plain=plain, cache_filters=True, threads=threads)
+                try:
+                    r, rows = _poisson_run(srv, qs, float("inf"), seed)
+                    st = srv.stats()
+                    r.update({"steps": st.steps, "busy_s": st.busy_s, "admit_s": st.admit_s, "scan_s": st.scan_s,
+                              "probe_device_s": st.probe_device_s, "peak_active": st.peak_active,
+                              "rows_scanned": st.rows_scanned})
+                finally:
+                    srv.close()
+                res["plain" if plain else "shared"] = r
+                res["rows_plain" if plain else "rows_shared"] = rows
+            exact = exact and res.pop("rows_plain") == res.pop("rows_shared")
+            res["speedup_vs_plain"] = res["shared"]["throughput_qps"] / max(res["plain"]["throughput_qps"], 1e-9)
+            runs.append(res)
+        ratios = [r["speedup_vs_plain"] for r in runs]
+        out["saturation"] = {"mixes": runs, "queries_per_mix": flood, "speedup_min": min(ratios),
+                             "speedup_mean": statistics.mean(ratios),
+                             "shared_qps_mean": statistics.mean(r["shared"]["throughput_qps"] for r in runs),
+                             "plain_qps_mean": statistics.mean(r["plain"]["throughput_qps"] for r in runs)}
     out["bit_exact_vs_plain"] = exact
     del dev
     return out
