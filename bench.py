@@ -1,10 +1,9 @@
 #!/usr/bin/env python
 """Benchmark: the 3-dimension LIP star join (SSB Q3.3 shape) on 120M fact rows.
 
-One step = one query through the engine, one kernel launch (sj_query_run): the
-dimension builds (predicate -> filter + PHT insert), the fused scan/filter/
-probe/aggregate and the group compaction -- the span the reference's
-time_query covers (src/ssb-jo/q33/0-lip.cu:216-278).
+One step = one query through the engine: dimension builds (predicate ->
+filter + PHT insert) and the fused scan/filter/probe/aggregate kernel, exactly
+the span the reference's time_query covers (src/ssb-jo/q33/0-lip.cu:216-278).
 Inputs (1.92 GB of fact columns) are resident in HBM and larger than the 126 MB
 L2, so no flush is needed between steps.
 
@@ -103,15 +102,15 @@ class ClockSampler:
 
 
 def _traffic_from_profiles(bpk: int):
-    """Per-launch DRAM bytes (read + write) of the fused query kernel, from the
-    committed ncu capture of one launch of this workload; (bytes, how) or (None, why)."""
+    """Per-launch DRAM bytes (read + write) of the probe kernel, from the committed
+    ncu capture of one launch of this workload; (bytes, how) or (None, why)."""
     path = os.path.join(ROOT, "profiles", "probe_traffic.json")
     try:
         with open(path) as f:
             rec = json.load(f)
     except Exception:
         return None, "no profiles/probe_traffic.json"
-    ent = rec.get(f"fused_bpk{bpk}")
+    ent = rec.get(f"bpk{bpk}")
     if not ent or not ent.get("fact_rows"):
         return None, f"no capture for bf_bits_per_key={bpk}"
     if ent["fact_rows"] == FACT_ROWS:
@@ -294,11 +293,10 @@ def run_engine(args):
     pq = eng.prepare(query, cols, FACT_ROWS)
 
     def step(ev=None):
-        # one query = one kernel launch: the dimension builds, the probe and the
-        # group compaction of sj_query_run's fused kernel
+        pq.build(sptr)
         if ev:
             ev[0].record(stream)
-        pq.run(sptr)
+        pq.probe(sptr)
         if ev:
             ev[1].record(stream)
 
@@ -315,8 +313,9 @@ def run_engine(args):
     torch.cuda.synchronize()
     result = pq.fetch(stream=sptr)
 
-    # the kernel's own duration: CUDA events around it on every PROBE_EVERY-th
-    # timed step (sampling keeps the event records out of most launch gaps)
+    # the probe's own duration: CUDA events around it on every PROBE_EVERY-th timed
+    # step (an event pair between the build and the probe costs about 7 us of a
+    # 0.2 ms step, so sampling keeps the instrumentation out of ms_per_step)
     probe_every = PROBE_EVERY if args.steps >= 4 * PROBE_EVERY else 1
     probe_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                 for _ in range(0, args.steps, probe_every)]
@@ -337,18 +336,6 @@ def run_engine(args):
     total_ms = start.elapsed_time(stop)
     probe_ms = statistics.mean(a.elapsed_time(b) for a, b in probe_ev)
     stats = pq.stats()
-    assert pq.fetch(stream=sptr) == result
-    # the split form beside it: the probe kernel alone after the build kernels
-    split = []
-    for _ in range(12):
-        pq.build(sptr)
-        a, c2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        pq.probe(sptr)
-        c2.record(stream)
-        torch.cuda.synchronize()
-        split.append(a.elapsed_time(c2))
-    split_probe_ms = statistics.median(split[2:])
     assert pq.fetch(stream=sptr) == result
 
     t = torch.tensor([total_ms, probe_ms], device=f"cuda:{local}", dtype=torch.float64)
@@ -375,20 +362,19 @@ def run_engine(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded SplitMix64)",
             "config": _config(args.bpk),
-            "kernel_ms": probe_ms, "kernel_ms_sampled_steps": len(probe_ev), "split_probe_ms": split_probe_ms,
+            "probe_ms": probe_ms, "probe_ms_sampled_steps": len(probe_ev),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_gbs": algorithmic, "algorithmic_frac": algorithmic / peak,
-                         "note": "the step's one kernel (fused build + probe + group compaction, sj_probe_kernel): "
-                                 "achieved = DRAM bytes (read + write) of one launch, "
+                         "note": "probe kernel (sj_probe_kernel): achieved = DRAM bytes (read + write) of one launch, "
                                  f"{traffic_how}, / its mean duration (CUDA events on the launch stream); "
                                  "algorithmic_* use the full-load model of 16 B per fact row (3 FK columns + "
                                  "revenue), which this sector-skipping probe does not read (the first column "
                                  f"densely, later columns only at survivor rows); peak: {peak_kind} copy "
                                  "bandwidth" if traffic else
-                                 "fused query kernel: no DRAM capture for this setting, so achieved uses the "
-                                 "16 B/row algorithmic model"},
-            "gpu_launches": args.steps,
+                                 "probe kernel: no DRAM capture for this setting, so achieved uses the 16 B/row "
+                                 "algorithmic model"},
+            "gpu_launches": 4 * args.steps,
             "groups": len(result), "groups_merged_ok": groups_ok,
             "stats": {"step_in": list(stats.step_in)[:6], "step_out": list(stats.step_out)[:6],
                       "bf_inserted": list(stats.bf_inserted)[:3], "bf_words": list(stats.bf_words)[:3],

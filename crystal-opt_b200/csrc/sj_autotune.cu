@@ -5,7 +5,7 @@
 // would).  Search order, each step keeping the best so far:
 //   1. filter kind   direct bitmap, per-dimension auto layout, 8 or 16 bits per
 //                    key -- with every join order when the order is searched too
-//   2. geometry      threads x rows per lane, then the shared-memory filter budget
+//   2. geometry      threads x rows per lane, then rows per stage x stages
 //   3. join order    (when not searched in 1) most selective first, or every
 //                    permutation; then bits set per key 1..4 and 4 / 8 / 16
 //                    bits per key for the chosen order and geometry
@@ -236,27 +236,35 @@ extern "C" sj_status sj_autotune(sj_engine* eng, sj_plan* plan, const sj_autotun
       for_orders(c, joint);
     }
   }
-  // 2. geometry: CTA size x rows per lane, then the shared-memory filter budget
+  // 2. geometry: CTA size x rows per lane, then rows per stage x stages
   {
     const sj_plan start = best;
-    const int shapes[][2] = {{1024, 16}, {1024, 8}, {768, 16}, {768, 8}, {512, 16}, {512, 8}};
-    const int st_threads = start.tune.threads ? start.tune.threads : 1024;
-    const int st_rpl = start.tune.compact_threshold ? start.tune.compact_threshold : 16;
+    const int shapes[][2] = {{256, 0}, {256, 16}, {512, 0}, {512, 16}, {768, 0}};
     for (auto& sh : shapes) {
-      if (sh[0] == st_threads && sh[1] == st_rpl) continue;
       sj_plan c = start;
       c.tune.threads = sh[0];
       c.tune.compact_threshold = sh[1];
+      c.tune.chunk_rows = 0;
+      c.tune.stages = 0;
+      if (c.tune.threads == start.tune.threads && c.tune.compact_threshold == start.tune.compact_threshold &&
+          start.tune.chunk_rows == 0 && start.tune.stages == 0)
+        continue;
       consider(c);
     }
     const sj_plan mid = best;
-    const int budgets[] = {48 * 1024, 96 * 1024, 144 * 1024};
-    for (int b : budgets) {
-      if (b == mid.tune.bf_smem_bytes) continue;
-      sj_plan c = mid;
-      c.tune.bf_smem_bytes = b;
-      consider(c);
-    }
+    const int threads = mid.tune.threads ? mid.tune.threads : 512;
+    const int rpl = (mid.tune.compact_threshold == 16 && threads <= 512) ? 16 : 8;
+    const int pass = (threads / 32 - 1) * 32 * rpl;
+    const int passes[] = {2, 4, 8};
+    const int stages[] = {2, 3, 4};
+    for (int np : passes)
+      for (int sg : stages) {
+        sj_plan c = mid;
+        c.tune.chunk_rows = np * pass;
+        c.tune.stages = sg;
+        if ((int64_t)c.tune.chunk_rows * 4 > (1 << 19)) continue;
+        consider(c);
+      }
   }
   // 3. join order (when not searched with the filter), then bits set per key
   //    and the other filter sizes for the chosen order and geometry

@@ -22,6 +22,10 @@
 #include "sj_internal.h"
 
 namespace sj {
+uint32_t probe_smem_bytes(const SjProbeGeom& g);
+cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_per_thread, cudaStream_t st,
+                         const L2Window& w, bool pdl);
+cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st, bool pdl);
 __global__ void sj_dim_scan(const __grid_constant__ SjPlanRt P);
 __global__ void sj_dim_insert(const __grid_constant__ SjPlanRt P);
 }  // namespace sj
@@ -191,6 +195,7 @@ struct sj_query {
   sj_plan plan;
   SjPlanRt rt;
   SjProbeGeom geom;
+  uint32_t rows_per_thread = 4;
   uint8_t* arena = nullptr;
   size_t arena_bytes = 0;
   size_t zero_bytes = 0;
@@ -198,9 +203,6 @@ struct sj_query {
   std::vector<uint32_t> in_bitmaps;  // host staging, SJ_MAX_DIMS x 128 words
   cudaEvent_t ev_start = nullptr, ev_built = nullptr, ev_probed = nullptr;
   bool built = false, probed = false;
-  // the arena's scan inputs (payload bitmaps, prologue counts, grid barrier) are
-  // zero, as a fused run leaves them; else the next fused run clears the arena
-  bool clean = false;
   cudaStream_t stream = nullptr;
   L2Window l2win;  // the probe's window over the hash tables and filters
 };
@@ -259,6 +261,65 @@ static sj_status validate_plan(const sj_plan* p) {
   return SJ_OK;
 }
 
+// Shrink the ring depth, the chunk, then the filter budget, until the layout fits the
+// shared memory of ctas_per_sm CTAs (1 KB per CTA is reserved by the runtime).
+static void fit_geom(sj_engine* eng, SjProbeGeom& g, uint32_t ctas_per_sm, uint32_t pass) {
+  const size_t limit = std::min<size_t>(eng->smem_optin, 233472 / std::max<uint32_t>(1, ctas_per_sm) - 1024);
+  g.smem_bytes = probe_smem_bytes(g);
+  while (g.smem_bytes > limit) {
+    if (g.stages > 2) --g.stages;
+    else if (g.chunk_rows > pass) g.chunk_rows -= pass;
+    else if (g.bf_smem_bytes >= 4096) g.bf_smem_bytes /= 2;
+    else if (g.bf_smem_bytes) g.bf_smem_bytes = 0;
+    else if (g.group_smem_cap > 64) g.group_smem_cap /= 2;
+    else break;
+    g.smem_bytes = probe_smem_bytes(g);
+  }
+}
+
+// Probe launch geometry.  tune.threads is the CTA size (256, 512 or 768): one
+// producer warp plus 7, 15 or 23 consumer warps (a multiple of four warps, so the
+// register file splits evenly over the SM's four sub-partitions).  A pass covers
+// 32 * rows_per_lane rows per consumer warp; a chunk is a whole number of passes
+// of every consumer warp.
+static void default_geom(sj_engine* eng, const sj_plan* p, SjProbeGeom& g, uint32_t& rpl) {
+  const sj_tuning& t = p->tune;
+  const uint32_t threads = t.threads ? (uint32_t)t.threads : 512u;
+  const uint32_t nwc = threads / 32 - 1;
+  g.threads = (nwc + 1) * 32;
+  rpl = (t.compact_threshold == 16 && nwc <= 15) ? 16u : 8u;
+  const uint32_t pass = nwc * 32 * rpl;
+  g.chunk_rows = t.chunk_rows ? (uint32_t)t.chunk_rows : 4 * pass;
+  if (g.chunk_rows % pass) g.chunk_rows = (g.chunk_rows / pass + 1) * pass;
+  g.stages = t.stages ? (uint32_t)t.stages : 2u;
+  g.bf_smem_bytes = t.bf_smem_bytes ? (uint32_t)t.bf_smem_bytes : 40u * 1024u;
+  g.group_smem_cap = 1024;
+  uint32_t q1 = 1;
+  while (q1 < 2 * 32 * rpl) q1 <<= 1;
+  g.q1_cap = q1;
+  g.q2_cap = 128;  // room for a two-survivors-per-lane Q1 round (64) over a partial Q2
+  g.reorder_period = 16;
+  const uint32_t per_sm = t.ctas_per_sm ? (uint32_t)t.ctas_per_sm : 1u;
+  g.grid = (uint32_t)eng->sm_count * per_sm;
+  fit_geom(eng, g, per_sm, pass);
+}
+
+static sj_status check_geom(sj_engine* eng, SjProbeGeom& g, uint32_t rpl) {
+  const uint32_t nwc = g.threads / 32 - 1;
+  const bool ok = ((nwc == 7 || nwc == 15) && (rpl == 8 || rpl == 16)) || (nwc == 23 && (rpl == 4 || rpl == 8));
+  if (!ok) return fail(SJ_ERR_INVALID_ARGUMENT, "%u consumer warps x %u rows per lane not built", nwc, rpl);
+  if (g.stages < 2 || g.stages > 16) return fail(SJ_ERR_INVALID_ARGUMENT, "stages=%u (2..16)", g.stages);
+  if (g.chunk_rows == 0 || g.chunk_rows % (nwc * 32 * rpl) || g.chunk_rows * 4u > (1u << 19))
+    return fail(SJ_ERR_INVALID_ARGUMENT, "chunk_rows=%u", g.chunk_rows);
+  if (g.q1_cap < 2 * 32 * rpl || (g.q1_cap & (g.q1_cap - 1)) || g.q2_cap < 64 || (g.q2_cap & (g.q2_cap - 1)))
+    return fail(SJ_ERR_INVALID_ARGUMENT, "queue capacities");
+  if (g.reorder_period < 2 * g.stages) g.reorder_period = 2 * g.stages;
+  g.smem_bytes = probe_smem_bytes(g);
+  if (g.smem_bytes > eng->smem_optin)
+    return fail(SJ_ERR_INVALID_ARGUMENT, "probe needs %u B shared memory (limit %zu)", g.smem_bytes, eng->smem_optin);
+  return SJ_OK;
+}
+
 extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_query** out) {
   if (!eng || !out) return fail(SJ_ERR_INVALID_ARGUMENT, "NULL engine/out");
   *out = nullptr;
@@ -272,12 +333,12 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
   if (p.row_end < 0) p.row_end = p.fact_rows;
   const bool bf_auto = p.bf_bits_per_key == SJ_BF_AUTO;
   const uint32_t bpk = bf_auto ? 0u : (uint32_t)p.bf_bits_per_key;  // auto: sized as the direct bitmap
-  uint32_t prefix_words = 0;
-  for (int d = 0; d < p.n_dims; ++d)
-    if (p.dims[d].group) prefix_words += (uint32_t)(((int64_t)p.dims[d].payload_max - p.dims[d].payload_min + 32) / 32);
-  if (const char* why = make_probe_geom(p.tune, (uint32_t)eng->sm_count, eng->smem_optin, prefix_words, &q->geom)) {
+  default_geom(eng, &p, q->geom, q->rows_per_thread);
+  if (p.tune.compact_threshold) { /* compaction rounds always use full CTAs */ }
+  st = check_geom(eng, q->geom, q->rows_per_thread);
+  if (st != SJ_OK) {
     delete q;
-    return fail(SJ_ERR_INVALID_ARGUMENT, "probe geometry: %s", why);
+    return st;
   }
 
   // ---- arena layout: zeroed region first, then uploaded / written-once data
@@ -426,34 +487,6 @@ extern "C" sj_status sj_query_build(sj_query* q, void* stream) {
   SJ_CUDA(launch_windowed(sj_dim_insert, grid, dim3(256), 4 * max_pwords, st, L2Window{}, true, q->rt));
   SJ_CUDA(cudaEventRecord(q->ev_built, st));
   q->built = true;
-  q->probed = false;
-  q->clean = false;  // the split build leaves its payload bitmaps set
-  q->stream = st;
-  return SJ_OK;
-}
-
-// Build, probe and group compaction in one cooperative launch of the probe
-// kernel (its fused form).  The first run after prepare, a split build or an
-// error clears the arena first; every other run finds it as the last run left it.
-// build_ms of the statistics is then the clearing alone, probe_ms the launch.
-extern "C" sj_status sj_query_run(sj_query* q, void* stream) {
-  SjNvtxRange nvtx_range("sj.query.run");
-  if (!q) return fail(SJ_ERR_INVALID_ARGUMENT, "NULL query");
-  cudaStream_t st = (cudaStream_t)stream;
-  SJ_CUDA(cudaSetDevice(q->eng->device));
-  SJ_CUDA(cudaEventRecord(q->ev_start, st));
-  if (!q->clean) SJ_CUDA(cudaMemsetAsync(q->arena, 0, q->zero_bytes, st));
-  SJ_CUDA(cudaEventRecord(q->ev_built, st));
-  const cudaError_t e = launch_probe(q->rt, q->geom, st, q->l2win, false, true);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    q->clean = false;
-    return fail(e == cudaErrorCooperativeLaunchTooLarge ? SJ_ERR_UNSUPPORTED : SJ_ERR_CUDA,
-                "fused query launch: %s", cudaGetErrorString(e));
-  }
-  SJ_CUDA(cudaEventRecord(q->ev_probed, st));
-  q->built = q->probed = true;
-  q->clean = true;
   q->stream = st;
   return SJ_OK;
 }
@@ -465,7 +498,7 @@ extern "C" sj_status sj_query_probe(sj_query* q, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   SJ_CUDA(cudaSetDevice(q->eng->device));
   if (q->rt.row_end > q->rt.row_begin) {
-    SJ_CUDA(launch_probe(q->rt, q->geom, st, q->l2win, true, false));
+    SJ_CUDA(launch_probe(q->rt, q->geom, q->rows_per_thread, st, q->l2win, true));
   }
   SJ_CUDA(launch_finalize(q->rt, (uint32_t)q->group_capacity, st, true));
   SJ_CUDA(cudaEventRecord(q->ev_probed, st));
@@ -489,7 +522,6 @@ extern "C" sj_status sj_query_fetch(sj_query* q, sj_group_row* out, int64_t cap,
   SjDesc desc;
   SJ_CUDA(cudaMemcpyAsync(&desc, q->rt.desc, sizeof(desc), cudaMemcpyDeviceToHost, st));
   SJ_CUDA(cudaStreamSynchronize(st));
-  if (desc.error_flags) q->clean = false;
   if (desc.error_flags & kErrWaitTimeout) return fail(SJ_ERR_TIMEOUT, "probe kernel: bounded wait expired");
   if (desc.error_flags & kErrPayloadDomain)
     return fail(SJ_ERR_INVALID_ARGUMENT, "a grouped payload lies outside [payload_min, payload_max]");
@@ -598,13 +630,8 @@ static sj_status run_query_whole(sj_engine* eng, const sj_plan& p, sj_group_row*
                                  cudaStream_t st, cudaEvent_t t1) {
   sj_query* q = nullptr;
   sj_status s = sj_query_prepare(eng, &p, &q);
-  if (s == SJ_OK) {
-    s = sj_query_run(q, st);
-    if (s == SJ_ERR_UNSUPPORTED) {  // no room for a cooperative launch: the split kernels
-      s = sj_query_build(q, st);
-      if (s == SJ_OK) s = sj_query_probe(q, st);
-    }
-  }
+  if (s == SJ_OK) s = sj_query_build(q, st);
+  if (s == SJ_OK) s = sj_query_probe(q, st);
   cudaEventRecord(t1, st);
   if (s == SJ_OK) s = sj_query_fetch(q, out, cap, n_out, st);
   if (q) sj_query_release(q);
@@ -653,7 +680,7 @@ static sj_status run_query_streamed(sj_engine* eng, sj_plan p, const int32_t* ho
       SjPlanRt rt = q->rt;
       rt.row_begin = (uint64_t)std::max<int64_t>(pb, b);
       rt.row_end = (uint64_t)pe;
-      if (ce == cudaSuccess) ce = launch_probe(rt, q->geom, st, q->l2win, false, false);
+      if (ce == cudaSuccess) ce = launch_probe(rt, q->geom, q->rows_per_thread, st, q->l2win, false);
       if (ce != cudaSuccess) s = fail(SJ_ERR_CUDA, "streamed probe: %s", cudaGetErrorString(ce));
       pb = pe;
     }

@@ -82,12 +82,6 @@ struct SjDesc {
   unsigned long long bf_probes[kMaxDims];
   unsigned long long bf_passes[kMaxDims];
   unsigned long long reorders;
-  // fused query kernel: qualifying counts of its build prologue (left zero after
-  // every run for the next one) and the grid barrier (self-resetting count,
-  // generation counter)
-  uint32_t scan_count[kMaxDims];
-  uint32_t bar_count;
-  uint32_t bar_gen;
 };
 
 // Runtime parameters of one dimension in the kernels.
@@ -134,24 +128,16 @@ struct SjPlanRt {
 
 // Launch geometry of the probe kernel.
 struct SjProbeGeom {
-  uint32_t threads;           // CTA size: 32 x scanning warps (512, 768 or 1024)
-  uint32_t rows_per_lane;     // fact rows each lane tests per pass (8 or 16)
-  uint32_t grid;              // CTAs (one per SM)
-  uint32_t bf_smem_bytes;     // shared memory for filters
+  uint32_t threads;
+  uint32_t chunk_rows;
+  uint32_t stages;
+  uint32_t grid;
+  uint32_t bf_smem_bytes;
   uint32_t group_smem_cap;    // groups kept in shared memory when n_groups <= this
   uint32_t q1_cap, q2_cap;    // power-of-two survivor ring sizes
-  uint32_t reorder_period;    // passes of warp 0 between adaptive re-rankings
-  uint32_t prefix_words;      // fused build: payload-bitmap prefix words of all grouped dims
+  uint32_t reorder_period;    // chunks between adaptive re-rankings
   uint32_t smem_bytes;        // total dynamic shared memory
 };
-
-// Host-side entry points of the probe (sj_probe.cu).
-uint32_t probe_smem_bytes(const SjProbeGeom& g);
-const char* make_probe_geom(const sj_tuning& t, uint32_t sm_count, size_t smem_optin, uint32_t prefix_words,
-                            SjProbeGeom* out);
-cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, cudaStream_t st, const L2Window& w, bool pdl,
-                         bool fused);
-cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st, bool pdl);
 
 // Slot of key k: (k - key_min) mod ht_len, computed as an unsigned 32-bit
 // offset (HASH, crystal/join.cuh:27).  In-range keys take the subtraction

@@ -77,36 +77,6 @@ cudaError_t launch_windowed(void (*kernel)(K...), dim3 grid, dim3 block, size_t 
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
 }
 
-// Cooperative launch (every CTA of the grid resident at once, or the launch
-// fails with an error) with the window as above: for kernels whose CTAs meet in
-// grid-wide barriers.
-template <typename... K, typename... A>
-cudaError_t launch_cooperative(void (*kernel)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                               const L2Window& w, A&&... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[2];
-  unsigned n = 0;
-  if (w.bytes) {
-    attr[n].id = cudaLaunchAttributeAccessPolicyWindow;
-    attr[n].val.accessPolicyWindow.base_ptr = const_cast<void*>(w.base);
-    attr[n].val.accessPolicyWindow.num_bytes = w.bytes;
-    attr[n].val.accessPolicyWindow.hitRatio = w.hit_ratio;
-    attr[n].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-    attr[n].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-    ++n;
-  }
-  attr[n].id = cudaLaunchAttributeCooperative;
-  attr[n].val.cooperative = 1;
-  ++n;
-  cfg.attrs = attr;
-  cfg.numAttrs = n;
-  return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
-}
-
 }  // namespace sj
 
 #endif  // SJ_L2_H

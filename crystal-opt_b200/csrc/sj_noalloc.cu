@@ -26,6 +26,10 @@
 #include "sj_internal.h"
 
 namespace sj {
+uint32_t probe_smem_bytes(const SjProbeGeom& g);
+cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_per_thread, cudaStream_t st,
+                         const L2Window& w, bool pdl);
+cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st, bool pdl);
 __global__ void sj_dim_scan(const __grid_constant__ SjPlanRt P);
 __global__ void sj_dim_insert(const __grid_constant__ SjPlanRt P);
 }  // namespace sj
@@ -202,12 +206,21 @@ extern "C" sj_status sj_ssb_q33_run_noalloc(int device, const int32_t* lo_orderd
   }
 
   SjProbeGeom g;
-  sj_tuning tune;
-  memset(&tune, 0, sizeof(tune));
-  const uint32_t prefix_words = (span[0] + 31) / 32 + (span[1] + 31) / 32 + (span[2] + 31) / 32;
-  if (const char* why = make_probe_geom(tune, (uint32_t)sms, (size_t)smem_optin, prefix_words, &g))
-    return na_fail(SJ_ERR_UNSUPPORTED, "probe geometry on device %d: %s", device, why);
+  memset(&g, 0, sizeof(g));
+  g.threads = 512;  // 15 consumer warps + 1 producer warp, 8 rows per lane
+  g.chunk_rows = 15360;
+  g.stages = 2;
+  g.bf_smem_bytes = 40u * 1024u;
   rt.bf_smem_budget = g.bf_smem_bytes;
+  g.group_smem_cap = 1024;
+  g.q1_cap = 512;
+  g.q2_cap = 128;  // room for a two-survivors-per-lane Q1 round (64) over a partial Q2
+  g.reorder_period = 16;
+  g.grid = (uint32_t)sms;
+  g.smem_bytes = probe_smem_bytes(g);
+  if (g.smem_bytes > (uint32_t)smem_optin)
+    return na_fail(SJ_ERR_UNSUPPORTED, "probe needs %u bytes of shared memory per block; device %d allows %d",
+                   g.smem_bytes, device, smem_optin);
 
   // ---- clear, upload the IN lists, build, probe, finalize, read back
   auto check = [&](cudaError_t ce, const char* what) -> sj_status {
@@ -228,7 +241,7 @@ extern "C" sj_status sj_ssb_q33_run_noalloc(int device, const int32_t* lo_orderd
   if ((s = check(cudaGetLastError(), "dimension scan")) != SJ_OK) return s;
   sj_dim_insert<<<grid, 256, 4 * ((250 + 31) / 32), st>>>(rt);
   if ((s = check(cudaGetLastError(), "dimension insert")) != SJ_OK) return s;
-  if (lo_len > 0 && (s = check(launch_probe(rt, g, st, L2Window{}, false, false), "probe")) != SJ_OK) return s;
+  if (lo_len > 0 && (s = check(launch_probe(rt, g, 8, st, L2Window{}, false), "probe")) != SJ_OK) return s;
   if ((s = check(launch_finalize(rt, (uint32_t)groups, st, false), "finalize")) != SJ_OK) return s;
   SjDesc desc;
   if ((s = check(cudaMemcpyAsync(&desc, rt.desc, sizeof(desc), cudaMemcpyDeviceToHost, st), "reading status")) != SJ_OK)

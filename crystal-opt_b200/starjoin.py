@@ -128,7 +128,6 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "sj_query_prepare": (C.c_int, [P, C.POINTER(SjPlan), C.POINTER(P)]),
         "sj_query_build": (C.c_int, [P, P]),
         "sj_query_probe": (C.c_int, [P, P]),
-        "sj_query_run": (C.c_int, [P, P]),
         "sj_query_fetch": (C.c_int, [P, C.POINTER(SjGroupRow), C.c_int64, C.POINTER(C.c_int64), P]),
         "sj_query_get_stats": (C.c_int, [P, C.POINTER(SjQueryStats)]),
         "sj_query_release": (None, [P]),
@@ -169,7 +168,7 @@ def exported_symbols() -> List[str]:
     """Entry points declared in include/starjoin.h that the library must export."""
     return [
         "sj_engine_create", "sj_engine_destroy", "sj_status_string", "sj_last_error",
-        "sj_device_sm_count", "sj_query_prepare", "sj_query_build", "sj_query_probe", "sj_query_run",
+        "sj_device_sm_count", "sj_query_prepare", "sj_query_build", "sj_query_probe",
         "sj_query_fetch", "sj_query_get_stats", "sj_query_release", "sj_run_plain",
         "sj_ssb_q33_run", "sj_bloom_test", "sj_gen_column_device", "sj_gen_rows_device", "sj_gen_column_host",
         "sj_ssb_q33_run_noalloc", "sj_noalloc_last_error", "sj_autotune",
@@ -641,10 +640,6 @@ class Query:
 
     def probe(self, stream=None):
         check(self.eng.lib.sj_query_probe(self.h, stream))
-
-    def run(self, stream=None):
-        """Build + probe + group compaction in one cooperative launch."""
-        check(self.eng.lib.sj_query_run(self.h, stream))
 
     def fetch(self, cap=1 << 20, stream=None):
         rows = (SjGroupRow * cap)()

@@ -16,8 +16,7 @@
  *                              Replaced by sj_query_build().
  *   - probe<128,4>             src/ssb-jo/q33/0-lip.cu:28-112 (BF probes in LIP
  *                              order, PHT probes, group atomicAdd).
- *                              Replaced by sj_query_probe(), or with the builds
- *                              and the group read-out by one sj_query_run().
+ *                              Replaced by sj_query_probe().
  *   - the reference's Q4.1 4-dimension LIP driver (src/ssb-jo/q41/0-lip.cu:28-131)
  *                              is the n_dims == 4 form of the same plan.
  *
@@ -96,12 +95,12 @@ typedef struct sj_dim {
 
 /* Launch geometry; 0 fields are chosen by the engine (or the autotuner cache). */
 typedef struct sj_tuning {
-  int32_t threads;            /* threads per CTA of the probe kernel: 512, 768 or 1024 (0: 1024) */
-  int32_t chunk_rows;         /* unused by the plain probe (kept for layout compatibility) */
-  int32_t stages;             /* unused by the plain probe (kept for layout compatibility) */
-  int32_t ctas_per_sm;        /* 0 or 1: the probe runs one CTA per SM */
-  int32_t compact_threshold;  /* fact rows each lane tests per pass: 8 or 16 (0: 16) */
-  int32_t bf_smem_bytes;      /* shared-memory budget for filters (0: all the queues leave, <= 192 KB) */
+  int32_t threads;            /* threads per CTA of the probe kernel (128..1024) */
+  int32_t chunk_rows;         /* fact rows per TMA stage (multiple of 4*threads) */
+  int32_t stages;             /* TMA ring depth (2..8) */
+  int32_t ctas_per_sm;        /* persistent CTAs per SM (1..4) */
+  int32_t compact_threshold;  /* survivors queued before a compaction round (0 = threads) */
+  int32_t bf_smem_bytes;      /* shared-memory budget for Bloom filters */
 } sj_tuning;
 
 typedef struct sj_plan {
@@ -168,13 +167,6 @@ sj_status sj_query_prepare(sj_engine* e, const sj_plan* plan, sj_query** out);
 sj_status sj_query_build(sj_query* q, void* stream);
 /* Fused scan -> LIP filters -> PHT probes -> group SUM (async on stream). */
 sj_status sj_query_probe(sj_query* q, void* stream);
-/* Build + probe + group compaction in ONE kernel launch (async on stream): the
- * probe kernel runs the dimension builds as its prologue and compacts the
- * groups at its end, its CTAs meeting in grid-wide barriers (a cooperative
- * launch, one CTA per SM).  Same results as build + probe; fetch as after a
- * probe.  SJ_ERR_UNSUPPORTED when the device cannot hold the whole grid at once
- * (e.g. shared with other work); build + probe then still work. */
-sj_status sj_query_run(sj_query* q, void* stream);
 /* Wait for the stream, copy the groups out (sorted by the grouped attrs in
  * dimension order).  SJ_ERR_CAPACITY if cap < groups (*n_out = groups). */
 sj_status sj_query_fetch(sj_query* q, sj_group_row* out, int64_t cap, int64_t* n_out, void* stream);

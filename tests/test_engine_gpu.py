@@ -108,71 +108,16 @@ def test_row_ranges_and_ragged_tails(sj, oracle, engine, small, begin, end):
     assert got == oracle.run(q, host)
 
 
-GEOMETRIES = [dict(threads=512), dict(threads=768), dict(threads=1024), dict(threads=512, compact_threshold=8),
-              dict(threads=768, compact_threshold=8), dict(threads=1024, compact_threshold=8),
-              dict(bf_smem_bytes=16), dict(bf_smem_bytes=4096), dict(bf_smem_bytes=9000)]
-
-
-@pytest.mark.parametrize("tune", GEOMETRIES)
+@pytest.mark.parametrize("tune", [dict(threads=256), dict(threads=768), dict(stages=2), dict(stages=12, chunk_rows=4096),
+                                  dict(chunk_rows=4096), dict(chunk_rows=16384, stages=3),
+                                  dict(bf_smem_bytes=0), dict(ctas_per_sm=2, stages=2, chunk_rows=4096)])
 def test_launch_geometry_does_not_change_results(sj, oracle, engine, small, tune):
-    """Every probe shape (512 / 768 / 1,024 threads x 8 / 16 rows per lane) and
-    filter budgets from none to partial, through the fused one-launch query
-    (sj_run_plain) and the split build + probe kernels."""
     host, dev = small
     want = oracle.run(sj.q33_query(SMALL), host)
     for lip, bpk in ((True, 16), (True, 0), (False, 0)):
         q = sj.q33_query(SMALL, order=(2, 1, 0), lip=lip, bf_bits_per_key=bpk)
         got, _ = engine.run(q, dev, SMALL.fact_rows, tune=tune)
         assert got == want, (tune, lip, bpk)
-        pq = engine.prepare(q, dev, SMALL.fact_rows, tune=tune)
-        try:
-            pq.build()
-            pq.probe()
-            assert pq.fetch() == want, (tune, lip, bpk, "split")
-        finally:
-            pq.release()
-
-
-def test_unbuilt_probe_shapes_are_refused(sj, engine, small):
-    _, dev = small
-    q = sj.q33_query(SMALL)
-    for tune in (dict(threads=256), dict(threads=640), dict(compact_threshold=12), dict(ctas_per_sm=2)):
-        with pytest.raises(sj.StarJoinError):
-            engine.prepare(q, dev, SMALL.fact_rows, tune=tune)
-
-
-def test_fused_and_split_runs_interleave(sj, oracle, engine, small):
-    """Repeated one-launch runs reuse the arena as the previous run left it; a
-    split build in between, a different predicate on the same columns, and the
-    statistics stay right."""
-    host, dev = small
-    q = sj.q33_query(SMALL, order=(1, 0, 2), adaptive=True)
-    want = oracle.run(q, host)
-    pq = engine.prepare(q, dev, SMALL.fact_rows)
-    try:
-        for k in range(3):
-            pq.run()
-            assert pq.fetch() == want, k
-            st = pq.stats()
-            assert st.rows_scanned == SMALL.fact_rows and st.groups == len(want)
-            assert st.step_in[0] == SMALL.fact_rows
-        pq.build()
-        pq.probe()
-        assert pq.fetch() == want
-        for k in range(2):
-            pq.run()
-            assert pq.fetch() == want, ("after split", k)
-    finally:
-        pq.release()
-    q2 = sj.q33_query(SMALL, cities=tuple(range(0, 250, 7)), bf_bits_per_key=16)
-    want2 = oracle.run(q2, host)
-    pq = engine.prepare(q2, dev, SMALL.fact_rows)
-    try:
-        for k in range(3):
-            pq.run()
-            assert pq.fetch() == want2, k
-    finally:
-        pq.release()
 
 
 def test_no_qualifying_rows_and_all_rows(sj, oracle, engine, small):
