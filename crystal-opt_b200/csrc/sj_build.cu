@@ -4,22 +4,30 @@
 // Replaces the reference's build_hashtable_{s,c,d} kernels
 // (src/ssb-jo/q33/0-lip.cu:114-203).  Two launches per query, each covering every
 // dimension (blockIdx.y = dim):
-//   sj_dim_scan   counts qualifying rows and marks their payloads in a bitmap over
-//                 the payload domain (the group-key dictionary);
+//   sj_dim_scan   clears the hash tables and filters, counts qualifying rows and
+//                 marks their payloads in a bitmap over the payload domain (the
+//                 group-key dictionary);
 //   sj_dim_insert sizes the filter from the count (bits per inserted key), ranks
 //                 payloads into dense group codes, and inserts qualifying rows into
 //                 the PHT ([key, code] slots, the reference's 2 x int32 layout) and
 //                 the filter.
 // Everything the probe needs (filter geometry, code counts, group strides, the
-// starting LIP order) is written to the query descriptor on the device.  The
-// fused query kernel (sj_probe.cu) runs the same steps (sj_build.cuh) as its
-// prologue; these kernels serve the split build / probe entry points.
+// starting LIP order) is written to the query descriptor on the device: no host
+// round trip, so a whole query can be captured in a CUDA graph.
 #include "sj_build.cuh"
 
 namespace sj {
 
 __global__ void __launch_bounds__(256) sj_dim_scan(const __grid_constant__ SjPlanRt P) {
   pdl_launch_dependents();  // sj_dim_insert may be scheduled; it waits for this grid
+  // clear the hash tables and filters sj_dim_insert fills (every block of the grid)
+  if (P.zero_tables_bytes) {
+    uint4* z = reinterpret_cast<uint4*>(P.zero_tables);
+    const uint64_t n = P.zero_tables_bytes / 16u;
+    const uint64_t nt = (uint64_t)gridDim.x * gridDim.y * blockDim.x;
+    for (uint64_t i = ((uint64_t)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += nt)
+      z[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
   const uint32_t d = blockIdx.y;
   if (d >= P.n_dims) return;
   SjDesc* desc = P.desc;

@@ -1,6 +1,6 @@
-// sj_build.cuh -- device-side pieces of the dimension build, shared by the
-// stand-alone build kernels (sj_build.cu) and the fused query kernel
-// (sj_probe.cu), which runs the same build as its prologue.
+// sj_build.cuh -- device-side pieces of the dimension build (sj_build.cu's
+// kernels): the predicate, the scan and insert loops over a dimension, the
+// payload-bitmap prefix and dictionary, group strides and the starting LIP order.
 //
 // They restate the reference's build_hashtable_{s,c,d} kernels
 // (src/ssb-jo/q33/0-lip.cu:114-203): BlockLoad(dim_val) -> BlockPred* ->

@@ -198,7 +198,9 @@ struct sj_query {
   uint32_t rows_per_thread = 4;
   uint8_t* arena = nullptr;
   size_t arena_bytes = 0;
-  size_t zero_bytes = 0;
+  size_t zero_bytes = 0;     // the whole zeroed region (first build, after an error)
+  size_t head_bytes = 0;     // descriptor and payload bitmaps: cleared by every build
+  bool groups_clean = false; // the group sums are zero (the compaction kernel leaves them so)
   uint64_t group_capacity = 0;
   std::vector<uint32_t> in_bitmaps;  // host staging, SJ_MAX_DIMS x 128 words
   cudaEvent_t ev_start = nullptr, ev_built = nullptr, ev_probed = nullptr;
@@ -341,7 +343,10 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
     return st;
   }
 
-  // ---- arena layout: zeroed region first, then uploaded / written-once data
+  // ---- arena layout: zeroed region first (the descriptor and payload bitmaps,
+  // cleared by every build's memset; the hash tables and filters, cleared by the
+  // scan kernel; the group sums, left zero by the compaction kernel), then
+  // uploaded / written-once data
   size_t off = 0;
   const size_t desc_off = off;
   off = align256(off + sizeof(SjDesc));
@@ -349,6 +354,17 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
       dict_off[SJ_MAX_DIMS];
   uint32_t bf_max_log2[SJ_MAX_DIMS];
   uint64_t groups = 1;
+  for (int d = 0; d < p.n_dims; ++d) {
+    const sj_dim& D = p.dims[d];
+    pbm_off[d] = off;
+    if (D.group) {
+      const uint64_t span = (uint64_t)((int64_t)D.payload_max - D.payload_min + 1);
+      off = align256(off + 4 * ((span + 31) / 32));
+      groups *= span;
+    }
+  }
+  q->head_bytes = off;
+  const size_t tables_off = off;
   for (int d = 0; d < p.n_dims; ++d) {
     const sj_dim& D = p.dims[d];
     ht_off[d] = off;
@@ -365,13 +381,8 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
     }
     bf_off[d] = off;
     off = align256(off + std::max<size_t>(bf_bytes, 16));
-    pbm_off[d] = off;
-    if (D.group) {
-      const uint64_t span = (uint64_t)((int64_t)D.payload_max - D.payload_min + 1);
-      off = align256(off + 4 * ((span + 31) / 32));
-      groups *= span;
-    }
   }
+  const size_t tables_bytes = off - tables_off;
   q->group_capacity = groups;
   const size_t gsum_off = off;
   off = align256(off + 8 * groups);
@@ -398,13 +409,15 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
                 cudaGetErrorString(e));
   }
 
-  // hash tables, filters and payload bitmaps lie in [ht_off[0], gsum_off) of the arena
-  q->l2win = l2_window(q->arena + ht_off[0], gsum_off - ht_off[0], eng->l2_persist_bytes, eng->l2_window_max);
+  // hash tables and filters lie in [tables_off, tables_off + tables_bytes) of the arena
+  q->l2win = l2_window(q->arena + tables_off, tables_bytes, eng->l2_persist_bytes, eng->l2_window_max);
 
   // ---- runtime parameters
   SjPlanRt& rt = q->rt;
   memset(&rt, 0, sizeof(rt));
   rt.desc = reinterpret_cast<SjDesc*>(q->arena + desc_off);
+  rt.zero_tables = q->arena + tables_off;
+  rt.zero_tables_bytes = tables_bytes;
   rt.measure = p.measure;
   rt.measure_sub = p.measure_sub;
   rt.g_sum = reinterpret_cast<unsigned long long*>(q->arena + gsum_off);
@@ -472,7 +485,11 @@ extern "C" sj_status sj_query_build(sj_query* q, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   SJ_CUDA(cudaSetDevice(q->eng->device));
   SJ_CUDA(cudaEventRecord(q->ev_start, st));
-  SJ_CUDA(cudaMemsetAsync(q->arena, 0, q->zero_bytes, st));
+  // the scan kernel clears the hash tables and filters, the compaction kernel
+  // leaves the group sums zero; the whole region is cleared only after prepare
+  // and after an error
+  SJ_CUDA(cudaMemsetAsync(q->arena, 0, q->groups_clean ? q->head_bytes : q->zero_bytes, st));
+  q->groups_clean = true;
   int64_t max_rows = 1;
   uint32_t max_pwords = 1;
   for (int d = 0; d < q->plan.n_dims; ++d) {
@@ -498,9 +515,11 @@ extern "C" sj_status sj_query_probe(sj_query* q, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   SJ_CUDA(cudaSetDevice(q->eng->device));
   if (q->rt.row_end > q->rt.row_begin) {
+    q->groups_clean = false;  // until the compaction kernel has cleared them again
     SJ_CUDA(launch_probe(q->rt, q->geom, q->rows_per_thread, st, q->l2win, true));
   }
   SJ_CUDA(launch_finalize(q->rt, (uint32_t)q->group_capacity, st, true));
+  q->groups_clean = true;
   SJ_CUDA(cudaEventRecord(q->ev_probed, st));
   q->probed = true;
   q->stream = st;
@@ -522,6 +541,7 @@ extern "C" sj_status sj_query_fetch(sj_query* q, sj_group_row* out, int64_t cap,
   SjDesc desc;
   SJ_CUDA(cudaMemcpyAsync(&desc, q->rt.desc, sizeof(desc), cudaMemcpyDeviceToHost, st));
   SJ_CUDA(cudaStreamSynchronize(st));
+  if (desc.error_flags) q->groups_clean = false;
   if (desc.error_flags & kErrWaitTimeout) return fail(SJ_ERR_TIMEOUT, "probe kernel: bounded wait expired");
   if (desc.error_flags & kErrPayloadDomain)
     return fail(SJ_ERR_INVALID_ARGUMENT, "a grouped payload lies outside [payload_min, payload_max]");

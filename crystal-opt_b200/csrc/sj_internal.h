@@ -112,6 +112,8 @@ struct SjDimRt {
 struct SjPlanRt {
   SjDimRt dim[kMaxDims];
   SjDesc* desc;
+  uint8_t* zero_tables;        // hash tables and filters, cleared by the scan kernel (16-byte multiple)
+  uint64_t zero_tables_bytes;  // 0: the caller cleared them
   const int32_t* measure;
   const int32_t* measure_sub;
   unsigned long long* g_sum;

@@ -238,14 +238,12 @@ struct Warp {
     return slot_fast(ld_stream(D.fact_fk + base_row + rel, pol_first), D.key_min, D.ht_len, D.fastmod_m);
   }
 
-  __device__ __forceinline__ void aggregate(uint32_t rel, const Vals4& cv) {
+  __device__ __forceinline__ void aggregate(int64_t m, const Vals4& cv) {
     uint32_t g = 0;
     if (0 < P.n_dims && P.dim[0].grouped) g += cv.v0 * c.group_stride[0];
     if (1 < P.n_dims && P.dim[1].grouped) g += cv.v1 * c.group_stride[1];
     if (2 < P.n_dims && P.dim[2].grouped) g += cv.v2 * c.group_stride[2];
     if (3 < P.n_dims && P.dim[3].grouped) g += cv.v3 * c.group_stride[3];
-    int64_t m = (int64_t)ld_stream(P.measure + base_row + rel, pol_first);
-    if (P.measure_sub) m -= (int64_t)ld_stream(P.measure_sub + base_row + rel, pol_first);
     if (c.groups_in_smem) {
       atomicAdd(&s_sum[g], (unsigned long long)m);
       atomicAdd(&s_cnt[g], 1u);
@@ -255,38 +253,100 @@ struct Warp {
     }
   }
 
-  // Steps [first, n) for one survivor, then the aggregate.  Slots / codes a step
-  // needs and that earlier steps did not leave in registers are recomputed.
-  __device__ __forceinline__ void finish(uint32_t ver, uint32_t first, uint32_t rel, uint32_t have, uint32_t coded,
-                                         Vals4 sv, Vals4 cv) {
+  // Steps [first, n) for the warp's live lanes, then the aggregate.  Every lane
+  // takes part (warp-synchronous).  The loads a row still needs go out together
+  // instead of one dependent chain per step: first the fact keys of every
+  // dimension still to be looked up and the measure, then every remaining
+  // filter word and PHT slot.  The tests are then evaluated in step order and
+  // each step's entries and passes counted with two ballots (one shared-memory
+  // atomic per warp and step), exactly as a step-by-step walk counts them; a row
+  // passes only if every step passes, so loading ahead changes the work, never
+  // the answer.
+  __device__ __forceinline__ void finish(uint32_t ver, uint32_t first, bool alive, uint32_t rel, uint32_t have,
+                                         uint32_t coded, Vals4 sv, Vals4 cv) {
     const uint32_t n = c.n_steps[ver];
-    for (uint32_t p = first; p < n; ++p) {
-      const uint32_t st = c.steps[ver][p];
-      const uint32_t d = st & 15u;
-      atomicAdd(&c.step_in[p], 1u);
-      if (!((have >> d) & 1u)) {
-        sv.set(d, slot_at(d, rel));
-        have |= 1u << d;
-      }
-      if ((st >> 4) == kStepBF) {
-        atomicAdd(&c.probes[d], 1u);
-        if (!bf_test(bfview(d), sv.get(d), pol_keep)) return;
-        atomicAdd(&c.passes[d], 1u);
-      } else {
-        const int2 e = ld_slot(P.dim[d].ht + sv.get(d), pol_keep);
-        if (e.x == 0) return;
-        cv.set(d, (uint32_t)e.y);
-        coded |= 1u << d;
-      }
-      atomicAdd(&c.step_out[p], 1u);
+    if (!__ballot_sync(0xffffffffu, alive)) return;
+    // 1. fact keys of the dimensions still needed (steps and grouping), and the measure
+    uint32_t need = 0;
+    for (uint32_t p = first; p < n; ++p) need |= 1u << (c.steps[ver][p] & 15u);
+    for (uint32_t d = 0; d < P.n_dims; ++d)
+      if (P.dim[d].grouped && !((coded >> d) & 1u)) need |= 1u << d;
+    need &= ~have;
+    int64_t mv = 0;
+    if (alive) {
+#pragma unroll
+      for (uint32_t d = 0; d < kMaxDims; ++d)
+        if ((need >> d) & 1u) sv.set(d, slot_at(d, rel));
+      mv = (int64_t)ld_stream(P.measure + base_row + rel, pol_first);
+      if (P.measure_sub) mv -= (int64_t)ld_stream(P.measure_sub + base_row + rel, pol_first);
     }
+    // 2. every remaining filter word / PHT slot
+    uint64_t raw[kMaxSteps];
+#pragma unroll
+    for (uint32_t p = 0; p < kMaxSteps; ++p) {
+      raw[p] = 0;
+      if (alive && p >= first && p < n) {
+        const uint32_t st = c.steps[ver][p], d = st & 15u;
+        const uint32_t sl = sv.get(d);
+        if ((st >> 4) == kStepBF) {
+          const BfView f = bfview(d);
+          if (f.mode == kBfDirect) {
+            const uint32_t w = sl >> 5;
+            raw[p] = f.smem ? lds_u32(f.smem + w * 4u)
+                            : ld_keep_u32(reinterpret_cast<const uint32_t*>(f.gptr) + w, pol_keep);
+          } else {
+            const uint32_t w = bf_word(sl, f.log2);
+            raw[p] = f.smem ? lds_u64(f.smem + w * 8u)
+                            : ld_keep_u64(reinterpret_cast<const uint64_t*>(f.gptr) + w, pol_keep);
+          }
+        } else {
+          const int2 e = ld_slot(P.dim[d].ht + sl, pol_keep);
+          raw[p] = ((uint64_t)(uint32_t)e.y << 32) | (uint32_t)e.x;
+        }
+      }
+    }
+    // 3. the tests in step order, counted as the plan walks them
+#pragma unroll
+    for (uint32_t p = 0; p < kMaxSteps; ++p) {
+      if (p < first || p >= n) continue;
+      const uint32_t in = __ballot_sync(0xffffffffu, alive);
+      if (!in) return;
+      const uint32_t st = c.steps[ver][p], d = st & 15u;
+      const bool is_bf = (st >> 4) == kStepBF;
+      bool pass = false;
+      if (alive) {
+        const uint32_t sl = sv.get(d);
+        if (is_bf) {
+          if (c.bf_mode[d] == kBfDirect) {
+            pass = ((uint32_t)raw[p] >> (sl & 31u)) & 1u;
+          } else {
+            const uint64_t m = bf_mask(sl, P.dim[d].bf_k);
+            pass = (raw[p] & m) == m;
+          }
+        } else {
+          pass = (uint32_t)raw[p] != 0u;
+          cv.set(d, (uint32_t)(raw[p] >> 32));
+          coded |= 1u << d;
+        }
+      }
+      const uint32_t out = __ballot_sync(0xffffffffu, pass);
+      if (lane == 0) {
+        atomicAdd(&c.step_in[p], (uint32_t)__popc(in));
+        atomicAdd(&c.step_out[p], (uint32_t)__popc(out));
+        if (is_bf) {
+          atomicAdd(&c.probes[d], (uint32_t)__popc(in));
+          atomicAdd(&c.passes[d], (uint32_t)__popc(out));
+        }
+      }
+      alive = pass;
+    }
+    if (!alive) return;
     // codes of grouped dimensions whose PHT probe passed in an earlier step
     for (uint32_t d = 0; d < P.n_dims; ++d) {
       if (!P.dim[d].grouped || ((coded >> d) & 1u)) continue;
-      const uint32_t s = ((have >> d) & 1u) ? sv.get(d) : slot_at(d, rel);
-      cv.set(d, (uint32_t)ld_slot(P.dim[d].ht + s, pol_keep).y);
+      cv.set(d, (uint32_t)ld_slot(P.dim[d].ht + sv.get(d), pol_keep).y);
     }
-    aggregate(rel, cv);
+    aggregate(mv, cv);
   }
 
   // Q1 entries [h1, h1 + cnt): step 1, then finish (plans of <= 2 steps) or
@@ -320,7 +380,7 @@ struct Warp {
     }
     const uint32_t m = __ballot_sync(0xffffffffu, pass);
     if (n <= 2) {
-      if (pass) finish(ver, 2, rel, have, coded, sv, cv);
+      finish(ver, 2, pass, rel, have, coded, sv, cv);
     } else {
       if (pass) {
         q2[(t2 + __popc(m & lanemask_lt())) & q2m] = rel;
@@ -386,7 +446,7 @@ struct Warp {
 
   __device__ __forceinline__ void q2_round(uint32_t ver, uint32_t cnt) {
     __syncwarp();
-    if (lane < cnt) finish(ver, 2, q2[(h2 + lane) & q2m], 0u, 0u, Vals4{0, 0, 0, 0}, Vals4{0, 0, 0, 0});
+    finish(ver, 2, lane < cnt, q2[(h2 + lane) & q2m], 0u, 0u, Vals4{0, 0, 0, 0}, Vals4{0, 0, 0, 0});
     h2 += cnt;
   }
 
@@ -509,7 +569,6 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
   static_assert(RPL % 4 == 0, "rows per lane must be a multiple of 4");
   constexpr uint32_t NT = (NWC + 1) * 32;
   pdl_launch_dependents();
-  pdl_wait();  // the build's descriptor, hash tables and filters are complete
   extern __shared__ __align__(128) uint8_t smem[];
   const SmemLayout L = probe_layout(G);
   int32_t* stage = reinterpret_cast<int32_t*>(smem + L.stage_off);
@@ -526,9 +585,26 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
   const uint32_t n_chunks = (uint32_t)((span + CH - 1) / CH);
   const uint32_t my_iters = (blockIdx.x < n_chunks) ? (n_chunks - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
 
-  // ---- setup (thread 0): plan steps, filter placement, mbarriers ----------
+  // ---- setup (thread 0): mbarriers; while the build may still run (programmatic
+  // dependent launch), an L2 prefetch of this CTA's first chunks of the column
+  // the plan's order tests first (the fact columns are inputs, never written);
+  // then, the build complete, the plan steps and filter placement ------------
   if (tid == 0) {
     memset(&c, 0, sizeof(Ctl));
+    for (uint32_t s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NWC);
+    }
+    mbar_fence_init();
+    const int32_t* col0 = P.dim[P.order[0]].fact_fk;
+    for (uint32_t it = 0; it < S && it < my_iters; ++it) {
+      const uint64_t start = base_row + (uint64_t)(blockIdx.x + it * gridDim.x) * CH;
+      const uint32_t bytes = (uint32_t)(min((uint64_t)CH, P.row_end - start) & ~3ull) * 4u;
+      if (bytes) bulk_prefetch_l2(col0 + start, bytes);
+    }
+  }
+  pdl_wait();  // the build's descriptor, hash tables and filters are complete
+  if (tid == 0) {
     for (uint32_t d = 0; d < P.n_dims; ++d) {
       c.bf_log2[d] = desc->dim[d].bf_log2;
       c.bf_mode[d] = desc->dim[d].bf_mode;
@@ -545,11 +621,6 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
     for (uint32_t d = 0; d < P.n_dims; ++d) c.group_stride[d] = desc->dim[d].group_stride;
     c.n_groups = desc->n_groups;
     c.groups_in_smem = c.n_groups <= G.group_smem_cap;
-    for (uint32_t s = 0; s < S; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], NWC);
-    }
-    mbar_fence_init();
   }
   __syncthreads();
 
@@ -762,7 +833,8 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
 }
 
 // Compact the non-empty groups into result rows, decoding dictionary codes back
-// to payload values.
+// to payload values, and clear each group it reads: the group sums are zero
+// again for the next probe, so no build has to clear the whole group space.
 __global__ void __launch_bounds__(256) sj_finalize_kernel(const __grid_constant__ SjPlanRt P) {
   pdl_wait();  // the probe's group sums are complete
   SjDesc* desc = P.desc;
@@ -783,6 +855,8 @@ __global__ void __launch_bounds__(256) sj_finalize_kernel(const __grid_constant_
     r.count = cnt;
     r.sum = P.g_sum[g];
     P.rows_out[pos] = r;
+    P.g_sum[g] = 0ull;
+    P.g_cnt[g] = 0ull;
   }
 }
 
@@ -820,7 +894,7 @@ cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_
 // pdl: the previous kernel of the stream is the probe (programmatic dependent launch).
 cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st, bool pdl) {
   uint32_t blocks = (group_capacity + 255) / 256;
-  if (blocks > 1184) blocks = 1184;
+  if (blocks > 296) blocks = 296;  // grid-stride over the dense groups (24 for Q3.3)
   if (blocks < 1) blocks = 1;
   return launch_windowed(sj_finalize_kernel, dim3(blocks), dim3(256), 0, st, L2Window{}, pdl, P);
 }

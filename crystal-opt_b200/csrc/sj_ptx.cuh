@@ -109,6 +109,12 @@ __device__ __forceinline__ uint64_t ld_keep_u64(const uint64_t* p, uint64_t pol)
   return v;
 }
 
+// Bulk prefetch of [src, src + bytes) into L2 (src 16-byte aligned, bytes a
+// multiple of 16); nothing waits for it.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(p));
 }
