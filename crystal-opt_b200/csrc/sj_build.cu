@@ -4,11 +4,11 @@
 // Replaces the reference's build_hashtable_{s,c,d} kernels
 // (src/ssb-jo/q33/0-lip.cu:114-203).  Two launches per query, each covering every
 // dimension (blockIdx.y = dim):
-//   sj_dim_scan   clears the hash tables and filters, counts qualifying rows and
-//                 marks their payloads in a bitmap over the payload domain (the
-//                 group-key dictionary);
+//   sj_dim_scan   clears the hash tables and filters, lists the qualifying rows
+//                 (their count sizes the filter) and marks their payloads in a
+//                 bitmap over the payload domain (the group-key dictionary);
 //   sj_dim_insert sizes the filter from the count (bits per inserted key), ranks
-//                 payloads into dense group codes, and inserts qualifying rows into
+//                 payloads into dense group codes, and inserts the listed rows into
 //                 the PHT ([key, code] slots, the reference's 2 x int32 layout) and
 //                 the filter.
 // Everything the probe needs (filter geometry, code counts, group strides, the
@@ -31,8 +31,7 @@ __global__ void __launch_bounds__(256) sj_dim_scan(const __grid_constant__ SjPla
   const uint32_t d = blockIdx.y;
   if (d >= P.n_dims) return;
   SjDesc* desc = P.desc;
-  const uint32_t count = dim_scan_rows(P, d, blockIdx.x, gridDim.x, &desc->error_flags);
-  if ((threadIdx.x & 31u) == 0 && count) atomicAdd(&desc->dim[d].n_inserted, count);
+  dim_scan_rows(P, d, blockIdx.x, gridDim.x, &desc->error_flags, &desc->dim[d].n_inserted);
 }
 
 __global__ void __launch_bounds__(256) sj_dim_insert(const __grid_constant__ SjPlanRt P) {
@@ -76,7 +75,7 @@ __global__ void __launch_bounds__(256) sj_dim_insert(const __grid_constant__ SjP
       choose_start(P, ins, desc->start_order, desc->bf_smem_off);
     }
   }
-  dim_insert_rows(P, d, mode, log2, prefix, blockIdx.x, gridDim.x);
+  dim_insert_rows(P, d, mode, log2, prefix, n_ins, blockIdx.x, gridDim.x);
 }
 
 }  // namespace sj

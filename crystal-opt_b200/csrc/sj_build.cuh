@@ -30,12 +30,12 @@ __device__ __forceinline__ bool dim_pred(const SjDimRt& D, uint64_t i) {
 }
 
 // Scan of dimension d by block `blk` of `nblk` (block-strided over the rows):
-// marks the payload of every qualifying row in the payload bitmap and returns
-// the calling warp's qualifying count (identical in all lanes).
-__device__ __forceinline__ uint32_t dim_scan_rows(const SjPlanRt& P, uint32_t d, uint32_t blk, uint32_t nblk,
-                                                  uint32_t* error_flags) {
+// marks the payload of every qualifying row in the payload bitmap and appends
+// the row's index to D.qual_rows, counted in *n_qual (one atomic per warp).
+__device__ __forceinline__ void dim_scan_rows(const SjPlanRt& P, uint32_t d, uint32_t blk, uint32_t nblk,
+                                              uint32_t* error_flags, uint32_t* n_qual) {
   const SjDimRt& D = P.dim[d];
-  uint32_t count = 0;
+  const uint32_t lane = threadIdx.x & 31u;
   for (uint64_t i0 = (uint64_t)blk * blockDim.x; i0 < D.rows; i0 += (uint64_t)nblk * blockDim.x) {
     const uint64_t i = i0 + threadIdx.x;
     const bool q = (i < D.rows) && dim_pred(D, i);
@@ -49,9 +49,14 @@ __device__ __forceinline__ uint32_t dim_scan_rows(const SjPlanRt& P, uint32_t d,
         if (!(*w & bit)) atomicOr(w, bit);
       }
     }
-    count += __popc(__ballot_sync(0xffffffffu, q));
+    const uint32_t m = __ballot_sync(0xffffffffu, q);
+    if (m) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(n_qual, (uint32_t)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (q) D.qual_rows[base + __popc(m & lanemask_lt())] = (uint32_t)i;
+    }
   }
-  return count;
 }
 
 // Exclusive prefix of the popcounts of `words` bitmap words into pre[] (and their
@@ -176,15 +181,17 @@ __device__ __forceinline__ void choose_start(const SjPlanRt& P, const uint32_t* 
   }
 }
 
-// Insert of dimension d by block `blk` of `nblk`: qualifying rows claim their
-// PHT slot (BlockBuildSelectivePHT_2: the key once, then the value -- here the
-// payload's dense code, its rank in the payload bitmap) and set their filter
-// bits, keyed by the PHT slot so the filter never rejects a row the PHT accepts.
+// Insert of dimension d by block `blk` of `nblk`, over the n_qual rows the scan
+// listed: each claims its PHT slot (BlockBuildSelectivePHT_2: the key once, then
+// the value -- here the payload's dense code, its rank in the payload bitmap)
+// and sets its filter bits, keyed by the PHT slot so the filter never rejects a
+// row the PHT accepts.
 __device__ __forceinline__ void dim_insert_rows(const SjPlanRt& P, uint32_t d, uint32_t mode, uint32_t log2,
-                                                const uint32_t* prefix, uint32_t blk, uint32_t nblk) {
+                                                const uint32_t* prefix, uint32_t n_qual, uint32_t blk,
+                                                uint32_t nblk) {
   const SjDimRt& D = P.dim[d];
-  for (uint64_t i = (uint64_t)blk * blockDim.x + threadIdx.x; i < D.rows; i += (uint64_t)nblk * blockDim.x) {
-    if (!dim_pred(D, i)) continue;
+  for (uint32_t k = blk * blockDim.x + threadIdx.x; k < n_qual; k += nblk * blockDim.x) {
+    const uint32_t i = D.qual_rows[k];
     const int32_t key = D.key[i];
     const uint32_t s = slot_of(key, D.key_min, D.ht_len, D.fastmod_m);
     int32_t val = 0;

@@ -351,7 +351,7 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
   const size_t desc_off = off;
   off = align256(off + sizeof(SjDesc));
   size_t ht_off[SJ_MAX_DIMS], bf_off[SJ_MAX_DIMS], pbm_off[SJ_MAX_DIMS], inbm_off[SJ_MAX_DIMS],
-      dict_off[SJ_MAX_DIMS];
+      dict_off[SJ_MAX_DIMS], qual_off[SJ_MAX_DIMS];
   uint32_t bf_max_log2[SJ_MAX_DIMS];
   uint64_t groups = 1;
   for (int d = 0; d < p.n_dims; ++d) {
@@ -395,6 +395,8 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
     off = align256(off + 4 * (SJ_MAX_IN_CODES / 32));
     dict_off[d] = off;
     if (D.group) off = align256(off + 4 * (size_t)((int64_t)D.payload_max - D.payload_min + 1));
+    qual_off[d] = off;
+    off = align256(off + 4 * (size_t)std::max<int64_t>(D.rows, 1));
   }
   const size_t rows_off = off;
   off = align256(off + sizeof(sj_group_row) * groups);
@@ -444,6 +446,7 @@ extern "C" sj_status sj_query_prepare(sj_engine* eng, const sj_plan* plan, sj_qu
     R.bf = q->arena + bf_off[d];
     R.payload_bitmap = reinterpret_cast<uint32_t*>(q->arena + pbm_off[d]);
     R.dict = reinterpret_cast<int32_t*>(q->arena + dict_off[d]);
+    R.qual_rows = reinterpret_cast<uint32_t*>(q->arena + qual_off[d]);
     R.rows = (uint64_t)D.rows;
     R.fastmod_m = ~0ull / (uint64_t)(uint32_t)D.ht_len + 1ull;
     R.key_min = D.key_min;
@@ -501,7 +504,9 @@ extern "C" sj_status sj_query_build(sj_query* q, void* stream) {
   dim3 grid(bx, (unsigned)q->plan.n_dims);
   sj_dim_scan<<<grid, 256, 0, st>>>(q->rt);
   SJ_CUDA(cudaGetLastError());
-  SJ_CUDA(launch_windowed(sj_dim_insert, grid, dim3(256), 4 * max_pwords, st, L2Window{}, true, q->rt));
+  // the insert walks only the listed qualifying rows: a smaller grid
+  const dim3 igrid(std::max(1u, std::min<uint32_t>(bx, (uint32_t)q->eng->sm_count * 2)), (unsigned)q->plan.n_dims);
+  SJ_CUDA(launch_windowed(sj_dim_insert, igrid, dim3(256), 4 * max_pwords, st, L2Window{}, true, q->rt));
   SJ_CUDA(cudaEventRecord(q->ev_built, st));
   q->built = true;
   q->stream = st;

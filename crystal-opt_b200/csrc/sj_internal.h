@@ -95,6 +95,7 @@ struct SjDimRt {
   void* bf;                   // filter words
   uint32_t* payload_bitmap;   // grouped: bitmap over the payload domain
   int32_t* dict;              // grouped: code -> payload
+  uint32_t* qual_rows;        // indices of the qualifying dimension rows (the scan appends, the insert reads)
   uint64_t rows;
   uint64_t fastmod_m;         // ceil(2^64 / ht_len) for the slot reduction
   int32_t key_min;

@@ -108,7 +108,7 @@ extern "C" sj_status sj_ssb_q33_run_noalloc(int device, const int32_t* lo_orderd
   size_t off = 0;
   const size_t desc_off = off;
   off = a256(off + sizeof(SjDesc));
-  size_t ht_off[3], bf_off[3], pbm_off[3], inbm_off[3], dict_off[3];
+  size_t ht_off[3], bf_off[3], pbm_off[3], inbm_off[3], dict_off[3], qual_off[3];
   uint32_t bf_log2[3];
   for (int d = 0; d < 3; ++d) {
     ht_off[d] = off;
@@ -137,6 +137,8 @@ extern "C" sj_status sj_ssb_q33_run_noalloc(int device, const int32_t* lo_orderd
     off = a256(off + 4 * (SJ_MAX_IN_CODES / 32));
     dict_off[d] = off;
     off = a256(off + 4 * (size_t)span[d]);
+    qual_off[d] = off;
+    off = a256(off + 4 * (size_t)rows[d]);
   }
   const size_t rows_off = off;
   off = a256(off + sizeof(sj_group_row) * groups);
@@ -189,6 +191,7 @@ extern "C" sj_status sj_ssb_q33_run_noalloc(int device, const int32_t* lo_orderd
     R.bf = base + bf_off[d];
     R.payload_bitmap = reinterpret_cast<uint32_t*>(base + pbm_off[d]);
     R.dict = reinterpret_cast<int32_t*>(base + dict_off[d]);
+    R.qual_rows = reinterpret_cast<uint32_t*>(base + qual_off[d]);
     R.rows = (uint64_t)rows[d];
     R.fastmod_m = ~0ull / (uint64_t)ht_len[d] + 1ull;
     R.key_min = key_min[d];

@@ -203,8 +203,8 @@ sj_status sj_ssb_q33_run(sj_engine* e,
  * every allocation).  No counterpart in the reference.  It allocates nothing: all
  * scratch (hash tables, filters, group partials, result rows) lives in one
  * 48 MiB file-scope device array that every GPU loading this library holds until
- * the process exits; queries needing more return SJ_ERR_CAPACITY (dimension
- * tables up to about 1.2M customer + supplier rows fit).  Column pointers are
+ * the process exits; queries needing more return SJ_ERR_CAPACITY (the
+ * customer and supplier tables together up to about 2.3M rows fit).  Column pointers are
  * device memory; `out` is a host buffer of `cap` rows.  Every call looks up
  * the array's device address with `device` current (the lookup allocates
  * nothing and stays valid across cudaDeviceReset); the first call on a device
