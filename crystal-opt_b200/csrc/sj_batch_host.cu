@@ -542,3 +542,93 @@ extern "C" sj_status sjb_batch_get_stats(sjb_batch* b, sjb_stats* out) {
   *out = b->last;
   return SJ_OK;
 }
+
+// ------------------------------------------------------------------ tuner ----
+// Probe shape of the batched form, chosen by timing: every candidate CTA size x
+// shared-memory group-partial budget runs the caller's sample batch on a batch
+// of its own (same schema, same other limits), `reps` times after one warm-up;
+// the median probe time (CUDA events around the probe) decides.  Every
+// candidate's groups must equal the first candidate's.
+namespace {
+bool row_less_b(const sjb_row& a, const sjb_row& b) {
+  if (a.query != b.query) return a.query < b.query;
+  for (int d = 0; d < SJ_MAX_DIMS; ++d)
+    if (a.attr[d] != b.attr[d]) return a.attr[d] < b.attr[d];
+  return false;
+}
+bool rows_same_b(std::vector<sjb_row> a, std::vector<sjb_row> b) {
+  if (a.size() != b.size()) return false;
+  std::sort(a.begin(), a.end(), row_less_b);
+  std::sort(b.begin(), b.end(), row_less_b);
+  for (size_t i = 0; i < a.size(); ++i)
+    if (a[i].query != b[i].query || a[i].count != b[i].count || a[i].sum != b[i].sum ||
+        memcmp(a[i].attr, b[i].attr, sizeof(a[i].attr)) != 0)
+      return false;
+  return true;
+}
+}  // namespace
+
+extern "C" sj_status sjb_batch_tune(sj_engine* eng, const sjb_schema* schema, const sjb_limits* base,
+                                    const sjb_query* sample, int32_t n, int32_t reps, sjb_limits* chosen,
+                                    sjb_tune_report* report) {
+  if (!eng || !schema || !sample || !chosen || n < 1 || n > SJB_MAX_QUERIES)
+    return fail_fmt(SJ_ERR_INVALID_ARGUMENT, "sjb_batch_tune: bad arguments");
+  if (reps < 1) reps = 3;
+  sjb_limits lim0;
+  memset(&lim0, 0, sizeof(lim0));
+  if (base) lim0 = *base;
+  sjb_tune_report rep;
+  memset(&rep, 0, sizeof(rep));
+  const int threads[] = {1024, 512, 256};
+  const int entries[] = {6144, 2048, 12288};
+  std::vector<sjb_row> first, rows;
+  float best = 3.4e38f;
+  sjb_limits best_lim = lim0;
+  for (int t : threads)
+    for (int e : entries) {
+      sjb_limits L = lim0;
+      L.threads = t;
+      L.smem_group_entries = e;
+      sjb_batch* b = nullptr;
+      if (sjb_batch_create(eng, schema, &L, &b) != SJ_OK) continue;  // a shape that does not fit
+      std::vector<float> ms;
+      sj_status st = SJ_OK;
+      for (int r = 0; r <= reps && st == SJ_OK; ++r) {
+        int64_t got = 0;
+        rows.resize(std::max<size_t>(rows.size(), 4096));
+        st = sjb_batch_run(b, sample, n, rows.data(), (int64_t)rows.size(), &got, nullptr);
+        if (st == SJ_ERR_CAPACITY && got > (int64_t)rows.size()) {  // more result rows than the buffer
+          rows.resize((size_t)got);
+          st = sjb_batch_run(b, sample, n, rows.data(), (int64_t)rows.size(), &got, nullptr);
+        }
+        if (st != SJ_OK) break;
+        if (r == 0) {  // warm-up run: the groups to compare
+          std::vector<sjb_row> mine(rows.begin(), rows.begin() + got);
+          if (first.empty() && rep.candidates == 0) first = mine;
+          else if (!rows_same_b(first, mine)) ++rep.mismatches;
+          continue;
+        }
+        sjb_stats s;
+        sjb_batch_get_stats(b, &s);
+        ms.push_back(s.ms_probe);
+      }
+      sjb_batch_destroy(b);
+      if (st != SJ_OK || ms.empty()) continue;
+      std::sort(ms.begin(), ms.end());
+      const float med = ms[ms.size() / 2];
+      if (rep.candidates == 0) rep.default_probe_ms = med;
+      ++rep.candidates;
+      if (med < best) {
+        best = med;
+        best_lim = L;
+      }
+    }
+  if (!rep.candidates) return fail_fmt(SJ_ERR_UNSUPPORTED, "sjb_batch_tune: no candidate shape ran");
+  rep.threads = best_lim.threads;
+  rep.smem_group_entries = best_lim.smem_group_entries;
+  rep.best_probe_ms = best;
+  *chosen = best_lim;
+  if (report) *report = rep;
+  if (rep.mismatches) return fail_fmt(SJ_ERR_CUDA, "sjb_batch_tune: %d candidate shapes changed the groups", rep.mismatches);
+  return SJ_OK;
+}

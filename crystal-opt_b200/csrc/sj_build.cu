@@ -62,17 +62,24 @@ __global__ void __launch_bounds__(256) sj_dim_insert(const __grid_constant__ SjP
       write_dict(D, prefix, pwords);
       if (threadIdx.x == 0) desc->dim[d].n_codes = s_total;
     }
-    if (d == 0 && threadIdx.x == 0) {
+    if (d == 0 && threadIdx.x < 32) {  // the query-wide fields, by warp 0
+      const uint32_t lane = threadIdx.x;
       uint32_t n_codes[kMaxDims] = {0, 0, 0, 0}, stride[kMaxDims], ins[kMaxDims] = {0, 0, 0, 0};
-      for (uint32_t e = 0; e < P.n_dims; ++e) {
+#pragma unroll
+      for (uint32_t e = 0; e < kMaxDims; ++e) {
+        if (e >= P.n_dims) continue;
         ins[e] = desc->dim[e].n_inserted;
         if (!P.dim[e].grouped) continue;
         const uint32_t ew = (P.dim[e].payload_span + 31u) / 32u;
-        for (uint32_t w = 0; w < ew; ++w) n_codes[e] += __popc(P.dim[e].payload_bitmap[w]);
+        uint32_t c = 0;
+        for (uint32_t w = lane; w < ew; w += 32) c += __popc(P.dim[e].payload_bitmap[w]);
+        n_codes[e] = __reduce_add_sync(0xffffffffu, c);
       }
-      desc->n_groups = group_strides(P, n_codes, stride);
-      for (uint32_t e = 0; e < P.n_dims; ++e) desc->dim[e].group_stride = stride[e];
-      choose_start(P, ins, desc->start_order, desc->bf_smem_off);
+      if (lane == 0) {
+        desc->n_groups = group_strides(P, n_codes, stride);
+        for (uint32_t e = 0; e < P.n_dims; ++e) desc->dim[e].group_stride = stride[e];
+      }
+      choose_start(P, ins, desc->start_order, desc->bf_smem_off, lane);
     }
   }
   dim_insert_rows(P, d, mode, log2, prefix, n_ins, blockIdx.x, gridDim.x);

@@ -113,71 +113,110 @@ __device__ __forceinline__ uint32_t group_strides(const SjPlanRt& P, const uint3
   return groups;
 }
 
-// Starting LIP order and filter placement for the probe.  Filters take the
-// probe's shared memory in LIP order while they fit.  With adaptive LIP the
-// order is the cheapest one over all permutations, with each dimension's
-// qualifying fraction as its pass-rate estimate; otherwise the plan's order.
-__device__ __forceinline__ void choose_start(const SjPlanRt& P, const uint32_t* inserted, uint32_t* start_order,
-                                             uint32_t* smem_off) {
+// Element i (0..3) of a 4-entry array held in registers.
+template <typename T>
+__device__ __forceinline__ T sel4(const T (&a)[kMaxDims], uint32_t i) {
+  return i == 0 ? a[0] : i == 1 ? a[1] : i == 2 ? a[2] : a[3];
+}
+
+// Permutation number p (0 <= p < n!) of 0..n-1 in lexicographic order, by the
+// factorial number system; entries from n on are left as their index.
+__device__ __forceinline__ void nth_perm(uint32_t p, uint32_t n, uint32_t (&perm)[kMaxDims]) {
+  uint32_t avail = (1u << n) - 1u;
+  uint32_t fact = n == 4 ? 6u : n == 3 ? 2u : 1u;  // (n-1)!
+#pragma unroll
+  for (uint32_t i = 0; i < kMaxDims; ++i) {
+    perm[i] = i;
+    if (i >= n) continue;
+    const uint32_t q = p / fact;
+    p -= q * fact;
+    uint32_t a = avail;
+    for (uint32_t k = 0; k < q; ++k) a &= a - 1u;  // the q-th unused dimension
+    perm[i] = (uint32_t)__ffs(a) - 1u;
+    avail &= ~(1u << perm[i]);
+    if (n - 1u - i > 1u) fact /= n - 1u - i;
+  }
+}
+
+// Starting LIP order and filter placement for the probe, by one warp (`lane`).
+// Filters take the probe's shared memory in LIP order while they fit.  With
+// adaptive LIP the order is the cheapest over all permutations (lane p prices
+// permutation p; ties go to the first in lexicographic order), with each
+// dimension's qualifying fraction as its pass-rate estimate; otherwise the
+// plan's order.
+__device__ __forceinline__ void choose_start(const SjPlanRt& P, const uint32_t (&inserted)[kMaxDims],
+                                             uint32_t* start_order, uint32_t* smem_off, uint32_t lane) {
   const uint32_t n = P.n_dims;
   uint32_t bytes[kMaxDims] = {0, 0, 0, 0};
   float rate[kMaxDims] = {1.f, 1.f, 1.f, 1.f};
-  for (uint32_t d = 0; d < n; ++d) {
+#pragma unroll
+  for (uint32_t d = 0; d < kMaxDims; ++d) {
+    if (d >= n) continue;
     const SjDimRt& D = P.dim[d];
     uint32_t l2;
     const uint32_t mode = bf_effective(D.bf_mode, D.bf_max_log2, D.bf_bits_per_key, inserted[d], P.bf_smem_budget, &l2);
     bytes[d] = (mode == kBfDirect) ? max(8u, (1u << l2) / 8u) : (8u << l2);
     rate[d] = ((float)inserted[d] + 1.f) / ((float)D.rows + 2.f);
   }
-  auto place = [&](const uint32_t* ord, uint32_t* off, float* weight) {
+  // placement of the filters for order `ord`: byte offsets and test weights
+  auto place = [&](const uint32_t (&ord)[kMaxDims], uint32_t (&off)[kMaxDims], float (&weight)[kMaxDims]) {
     uint32_t used = 0;
-    for (uint32_t p = 0; p < n; ++p) {
-      const uint32_t d = ord[p];
-      const bool fits = P.lip && used + bytes[d] <= P.bf_smem_budget;
-      off[d] = fits ? used : ~0u;
-      weight[d] = fits ? 1.f : kL2TestCost;
-      if (fits) used += (bytes[d] + 15u) & ~15u;
+#pragma unroll
+    for (uint32_t d = 0; d < kMaxDims; ++d) {
+      off[d] = ~0u;
+      weight[d] = kL2TestCost;
+    }
+#pragma unroll
+    for (uint32_t p = 0; p < kMaxDims; ++p) {
+      if (p >= n) continue;
+      const uint32_t d = ord[p], b = sel4(bytes, d);
+      const bool fits = P.lip && used + b <= P.bf_smem_budget;
+#pragma unroll
+      for (uint32_t e = 0; e < kMaxDims; ++e)
+        if (e == d) {
+          off[e] = fits ? used : ~0u;
+          weight[e] = fits ? 1.f : kL2TestCost;
+        }
+      if (fits) used += (b + 15u) & ~15u;
     }
   };
   uint32_t best[kMaxDims] = {0, 1, 2, 3};
-  for (uint32_t p = 0; p < n; ++p) best[p] = P.order[p];
+#pragma unroll
+  for (uint32_t p = 0; p < kMaxDims; ++p)
+    if (p < n) best[p] = P.order[p];
   if (P.lip && P.adaptive && n > 1) {
-    uint32_t perm[kMaxDims] = {0, 1, 2, 3};
-    float best_cost = 3.4e38f;
-    for (;;) {
-      uint32_t off[kMaxDims];
-      float weight[kMaxDims];
-      place(perm, off, weight);
-      float cost = 0.f, live = 1.f;
-      for (uint32_t p = 0; p < n; ++p) {
-        cost += live * weight[perm[p]];
-        live *= rate[perm[p]];
-      }
-      if (cost < best_cost) {
-        best_cost = cost;
-        for (uint32_t p = 0; p < n; ++p) best[p] = perm[p];
-      }
-      int i = (int)n - 2;  // next permutation (lexicographic)
-      while (i >= 0 && perm[i] >= perm[i + 1]) --i;
-      if (i < 0) break;
-      int j = (int)n - 1;
-      while (perm[j] <= perm[i]) --j;
-      uint32_t t = perm[i];
-      perm[i] = perm[j];
-      perm[j] = t;
-      for (int a = i + 1, b = (int)n - 1; a < b; ++a, --b) {
-        t = perm[a];
-        perm[a] = perm[b];
-        perm[b] = t;
+    const uint32_t n_perm = n == 4 ? 24u : n == 3 ? 6u : 2u;
+    uint32_t perm[kMaxDims];
+    nth_perm(lane < n_perm ? lane : 0u, n, perm);
+    uint32_t off[kMaxDims];
+    float weight[kMaxDims];
+    place(perm, off, weight);
+    float cost = 0.f, live = 1.f;
+#pragma unroll
+    for (uint32_t p = 0; p < kMaxDims; ++p) {
+      if (p >= n) continue;
+      cost += live * sel4(weight, perm[p]);
+      live *= sel4(rate, perm[p]);
+    }
+    if (lane >= n_perm) cost = 3.4e38f;
+    uint32_t arg = lane;
+#pragma unroll
+    for (uint32_t o = 16; o; o >>= 1) {
+      const float c2 = __shfl_xor_sync(0xffffffffu, cost, o);
+      const uint32_t a2 = __shfl_xor_sync(0xffffffffu, arg, o);
+      if (c2 < cost || (c2 == cost && a2 < arg)) {
+        cost = c2;
+        arg = a2;
       }
     }
+    nth_perm(arg, n, best);
   }
-  uint32_t off[kMaxDims] = {~0u, ~0u, ~0u, ~0u};
+  uint32_t off[kMaxDims];
   float weight[kMaxDims];
   place(best, off, weight);
-  for (uint32_t d = 0; d < kMaxDims; ++d) {
-    start_order[d] = d < n ? best[d] : 0u;
-    smem_off[d] = d < n ? off[d] : ~0u;
+  if (lane < kMaxDims) {
+    start_order[lane] = lane < n ? sel4(best, lane) : 0u;
+    smem_off[lane] = lane < n ? sel4(off, lane) : ~0u;
   }
 }
 

@@ -205,6 +205,7 @@ struct sj_query {
   std::vector<uint32_t> in_bitmaps;  // host staging, SJ_MAX_DIMS x 128 words
   cudaEvent_t ev_start = nullptr, ev_built = nullptr, ev_probed = nullptr;
   bool built = false, probed = false;
+  bool probed_since_build = false;  // a further probe clears the probe's counters and the result count first
   cudaStream_t stream = nullptr;
   L2Window l2win;  // the probe's window over the hash tables and filters
 };
@@ -509,6 +510,7 @@ extern "C" sj_status sj_query_build(sj_query* q, void* stream) {
   SJ_CUDA(launch_windowed(sj_dim_insert, igrid, dim3(256), 4 * max_pwords, st, L2Window{}, true, q->rt));
   SJ_CUDA(cudaEventRecord(q->ev_built, st));
   q->built = true;
+  q->probed_since_build = false;
   q->stream = st;
   return SJ_OK;
 }
@@ -519,9 +521,15 @@ extern "C" sj_status sj_query_probe(sj_query* q, void* stream) {
   if (!q->built) return fail(SJ_ERR_INVALID_ARGUMENT, "probe before build");
   cudaStream_t st = (cudaStream_t)stream;
   SJ_CUDA(cudaSetDevice(q->eng->device));
+  const bool again = q->probed_since_build;
+  if (again) {  // probe again over the same build: counters and result rows start over
+    const size_t first = offsetof(SjDesc, groups_out);
+    SJ_CUDA(cudaMemsetAsync(reinterpret_cast<uint8_t*>(q->rt.desc) + first, 0, sizeof(SjDesc) - first, st));
+  }
+  q->probed_since_build = true;
   if (q->rt.row_end > q->rt.row_begin) {
     q->groups_clean = false;  // until the compaction kernel has cleared them again
-    SJ_CUDA(launch_probe(q->rt, q->geom, q->rows_per_thread, st, q->l2win, true));
+    SJ_CUDA(launch_probe(q->rt, q->geom, q->rows_per_thread, st, q->l2win, !again));  // after the insert kernel
   }
   SJ_CUDA(launch_finalize(q->rt, (uint32_t)q->group_capacity, st, true));
   q->groups_clean = true;

@@ -843,6 +843,7 @@ __global__ void __launch_bounds__(256) sj_finalize_kernel(const __grid_constant_
     const unsigned long long cnt = P.g_cnt[g];
     if (!cnt) continue;
     const uint32_t pos = atomicAdd(&desc->groups_out, 1u);
+    if (pos >= P.group_capacity) continue;  // cannot happen: at most n_groups rows
     sj_group_row r;
     for (uint32_t d = 0; d < kMaxDims; ++d) {
       r.attr[d] = 0;

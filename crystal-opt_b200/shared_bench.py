@@ -67,13 +67,25 @@ class PlainRunner:
         return out, dev_ms, wall
 
 
+def _tuned(eng: sj.Engine, sc: sj.StarSchema, dev, sample, threads: int, tune: bool):
+    """The probe shape for the batched and served forms: sjb_batch_tune on a
+    sample batch (outside every timed region) unless `threads` fixes it."""
+    if threads or not tune:
+        return {"threads": threads, "smem_group_entries": 0}, None
+    shape, rep = ss.tune_batch(eng, sc, dev, sample, reps=3)
+    return shape, {"candidates": rep.candidates, "mismatches": rep.mismatches, "threads": rep.threads,
+                   "smem_group_entries": rep.smem_group_entries, "best_probe_ms": rep.best_probe_ms,
+                   "default_probe_ms": rep.default_probe_ms}
+
+
 def batched(eng: sj.Engine, n_batches: int = 6, per_batch: int = 64, seed: int = 2024,
-            schema: Dict[str, int] = None, threads: int = 0) -> Dict[str, Any]:
+            schema: Dict[str, int] = None, threads: int = 0, tune: bool = True) -> Dict[str, Any]:
     sc = sj.StarSchema(**(schema or BATCH_SCHEMA))
     dev = sj.gen_device(sc)
     rng = random.Random(seed)
     batches = [[ss.random_query(rng, sc) for _ in range(per_batch)] for _ in range(n_batches + 2)]
-    b = ss.Batch(eng, sc, dev, use_graph=True, cache_filters=False, threads=threads)
+    shape, tuning = _tuned(eng, sc, dev, batches[0], threads, tune)
+    b = ss.Batch(eng, sc, dev, use_graph=True, cache_filters=False, **shape)
     try:
         for qs in batches[:2]:  # warm-up: graph instantiation, first touches
             b.run_raw(b.describe(qs))
@@ -111,14 +123,14 @@ def batched(eng: sj.Engine, n_batches: int = 6, per_batch: int = 64, seed: int =
         "workload": f"{per_batch} queries/batch, 2-4 dims, selectivity log-uniform [0.05%, 60%], "
                     f"row range log-uniform [1M, {sc.fact_rows // 1_000_000}M], fact {sc.fact_rows} rows",
         "queries_per_s": qps_dev, "queries_per_s_wall": qps_wall,
-        "ms_per_batch": statistics.mean(dev_ms), "probe_ms_per_batch": probe,
+        "ms_per_batch": statistics.mean(dev_ms), "ms_per_batch_each": dev_ms, "probe_ms_per_batch": probe,
         "plain_queries_per_s": plain_qps_dev, "plain_queries_per_s_wall": plain_qps_wall,
         "plain_ms_per_batch": statistics.mean(plain_dev),
         "speedup_vs_plain": qps_dev / plain_qps_dev, "speedup_vs_plain_wall": qps_wall / plain_qps_wall,
         "bit_exact_vs_plain": exact, "batches_timed": n_batches,
         "shared_scan_rows": statistics.mean(rows_read), "sum_of_query_ranges": sum_ranges,
         "probe_hbm_gbs_algorithmic": BYTES_PER_ROW_4DIM * statistics.mean(rows_read) / (probe / 1e3) / 1e9,
-        "cuda_graph": True, "filters_cached": False,
+        "cuda_graph": True, "filters_cached": False, "probe_shape": shape, "tuning": tuning,
     }
 
 
@@ -156,9 +168,11 @@ def _poisson_run(srv: ss.Server, queries: List[Dict[str, Any]], rate: float, see
 
 def serving(eng: sj.Engine, rates=(50.0, 200.0, 2000.0), seconds: float = 1.0, seed: int = 77,
             schema: Dict[str, int] = None, plain_cap: int = 300, flood: int = 2048, mixes: int = 3,
-            threads: int = 0) -> Dict[str, Any]:
+            threads: int = 0, tune: bool = True) -> Dict[str, Any]:
     sc = sj.StarSchema(**(schema or SERVE_SCHEMA))
     dev = sj.gen_device(sc)
+    trng = random.Random(seed + 5)
+    shape, tuning = _tuned(eng, sc, dev, [ss.random_query(trng, sc) for _ in range(64)], threads, tune)
     rng = random.Random(seed)
     out: Dict[str, Any] = {"workload": f"Poisson arrivals, 2-4 dims, selectivity log-uniform [0.05%, 60%], row "
                                        f"range log-uniform [1M, {sc.fact_rows // 1_000_000}M], resident fact "
@@ -167,7 +181,7 @@ def serving(eng: sj.Engine, rates=(50.0, 200.0, 2000.0), seconds: float = 1.0, s
     for i, rate in enumerate(rates):
         n = max(20, int(rate * seconds))
         qs = [ss.random_query(rng, sc) for _ in range(n)]
-        srv = ss.Server(eng, sc, dev, cache_filters=True, threads=threads)
+        srv = ss.Server(eng, sc, dev, cache_filters=True, **shape)
         try:
             warm = [ss.random_query(random.Random(seed + 1000 + i), sc) for _ in range(8)]
             for t in [srv.submit(q) for q in warm]:
@@ -179,7 +193,7 @@ def serving(eng: sj.Engine, rates=(50.0, 200.0, 2000.0), seconds: float = 1.0, s
         finally:
             srv.close()
         # the same arrivals with lone queries sent through the plain engine
-        srv = ss.Server(eng, sc, dev, cache_filters=True, threads=threads, solo_plain=True)
+        srv = ss.Server(eng, sc, dev, cache_filters=True, solo_plain=True, **shape)
         try:
             for t in [srv.submit(q) for q in warm]:
                 srv.wait(t, timeout_s=600.0)
@@ -206,7 +220,7 @@ def serving(eng: sj.Engine, rates=(50.0, 200.0, 2000.0), seconds: float = 1.0, s
             qs = [ss.random_query(mrng, sc) for _ in range(flood)]
             res = {"seed": seed * 1009 + mix}
             for plain in (False, True):
-                srv = ss.Server(eng, sc, dev, plain=plain, cache_filters=True, threads=threads)
+                srv = ss.Server(eng, sc, dev, plain=plain, cache_filters=True, **shape)
                 try:
                     r, rows = _poisson_run(srv, qs, float("inf"), seed)
                     st = srv.stats()
@@ -226,5 +240,6 @@ def serving(eng: sj.Engine, rates=(50.0, 200.0, 2000.0), seconds: float = 1.0, s
                              "shared_qps_mean": statistics.mean(r["shared"]["throughput_qps"] for r in runs),
                              "plain_qps_mean": statistics.mean(r["plain"]["throughput_qps"] for r in runs)}
     out["bit_exact_vs_plain"] = exact
+    out["probe_shape"], out["tuning"] = shape, tuning
     del dev
     return out

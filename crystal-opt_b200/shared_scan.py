@@ -78,7 +78,12 @@ class SjsStats(C.Structure):
                 ("probe_device_s", C.c_double), ("solo", C.c_uint64)]
 
 
-SYMBOLS = ["sjb_batch_create", "sjb_batch_destroy", "sjb_batch_run", "sjb_batch_get_stats",
+class SjbTuneReport(C.Structure):
+    _fields_ = [("candidates", C.c_int32), ("mismatches", C.c_int32), ("threads", C.c_int32),
+                ("smem_group_entries", C.c_int32), ("best_probe_ms", C.c_float), ("default_probe_ms", C.c_float)]
+
+
+SYMBOLS = ["sjb_batch_create", "sjb_batch_destroy", "sjb_batch_run", "sjb_batch_get_stats", "sjb_batch_tune",
            "sjs_server_create", "sjs_submit", "sjs_poll", "sjs_wait", "sjs_cancel", "sjs_get_stats", "sjs_now",
            "sjs_server_destroy"]
 
@@ -94,6 +99,8 @@ def load() -> C.CDLL:
         "sjb_batch_run": (C.c_int, [P, C.POINTER(SjbQuery), C.c_int32, C.POINTER(SjbRow), C.c_int64,
                                     C.POINTER(C.c_int64), P]),
         "sjb_batch_get_stats": (C.c_int, [P, C.POINTER(SjbStats)]),
+        "sjb_batch_tune": (C.c_int, [P, C.POINTER(SjbSchema), C.POINTER(SjbLimits), C.POINTER(SjbQuery), C.c_int32,
+                                     C.c_int32, C.POINTER(SjbLimits), C.POINTER(SjbTuneReport)]),
         "sjs_server_create": (C.c_int, [P, C.POINTER(SjbSchema), C.POINTER(SjsConfig), C.POINTER(P)]),
         "sjs_submit": (C.c_int, [P, C.POINTER(SjbQuery), C.POINTER(C.c_uint64)]),
         "sjs_poll": (C.c_int, [P, C.c_uint64, C.POINTER(SjsTicketInfo), C.POINTER(SjbRow), C.c_int64]),
@@ -373,18 +380,36 @@ class Batch:
             pass
 
 
+def tune_batch(eng: sj.Engine, schema: sj.StarSchema, cols: Dict[str, Any], queries: Sequence[Dict[str, Any]],
+               reps: int = 3, use_graph=True, cache_filters=False, dims=None, measure_sub: Optional[str] = None):
+    """sjb_batch_tune on a sample batch: returns ({"threads", "smem_group_entries"},
+    SjbTuneReport) -- the probe shape to pass to Batch / Server."""
+    lib = load()
+    sch, keep = make_schema(schema, cols, dims, measure_sub)
+    base = SjbLimits(0, 0, 0, 1 if use_graph else 0, 1 if cache_filters else 0, 0, 0)
+    arr = (SjbQuery * len(queries))()
+    qkeep: list = []
+    for i, q in enumerate(queries):
+        fill_query(q, arr[i], qkeep)
+    chosen, rep = SjbLimits(), SjbTuneReport()
+    sj.check(lib.sjb_batch_tune(eng.h, C.byref(sch), C.byref(base), arr, len(queries), reps, C.byref(chosen),
+                                C.byref(rep)))
+    return {"threads": chosen.threads, "smem_group_entries": chosen.smem_group_entries}, rep
+
+
 # ----------------------------------------------------------------- serving ----
 class Server:
     """The serving loop: submit() from any thread, wait()/poll() for results."""
 
     def __init__(self, eng: sj.Engine, schema: sj.StarSchema, cols: Dict[str, Any], plain=False, step_rows=0,
                  max_active=0, cache_filters=True, group_entries=0, filter_cache_bytes=0, threads=0,
-                 hbm_reserve_bytes=0, fault_admit_every=0, solo_plain=False):
+                 hbm_reserve_bytes=0, fault_admit_every=0, solo_plain=False, smem_group_entries=0):
         self.lib = load()
         self.eng, self.schema = eng, schema
         self._schema, self._keep = make_schema(schema, cols)
         cfg = SjsConfig()
-        cfg.limits = SjbLimits(group_entries, 0, filter_cache_bytes, 0, 1 if cache_filters else 0, threads, 0)
+        cfg.limits = SjbLimits(group_entries, 0, filter_cache_bytes, 0, 1 if cache_filters else 0, threads,
+                               smem_group_entries)
         cfg.step_rows = step_rows
         cfg.max_active = max_active
         cfg.plain = 1 if plain else 0

@@ -123,6 +123,26 @@ sj_status sjb_batch_run(sjb_batch* b, const sjb_query* queries, int32_t n, sjb_r
                         int64_t* n_out, void* stream);
 sj_status sjb_batch_get_stats(sjb_batch* b, sjb_stats* out);
 
+/* Autotuner of the batched form's probe shape (no counterpart in the
+ * reference, which fixes its launch shapes at compile time,
+ * src/ssb-jo/q33/0-lip.cu:245,268): runs `sample` (n queries) on a batch of
+ * each candidate shape -- CTA size 1024 / 512 / 256 threads x shared-memory
+ * group partials 6144 / 2048 / 12288 entries, the other limits from `base` --
+ * times the probe (median of `reps` runs after one warm-up) and returns the
+ * fastest shape's limits in *chosen.  Every candidate's groups must equal the
+ * first candidate's (SJ_ERR_CUDA otherwise).  Synchronous; the default stream. */
+typedef struct sjb_tune_report {
+  int32_t candidates;                /* shapes timed */
+  int32_t mismatches;                /* shapes whose groups differed (must be 0) */
+  int32_t threads;                   /* chosen CTA size */
+  int32_t smem_group_entries;        /* chosen shared-memory group partials */
+  float best_probe_ms;               /* chosen shape's median probe time */
+  float default_probe_ms;            /* the default shape's (1024 threads, 6144 entries) */
+} sjb_tune_report;
+sj_status sjb_batch_tune(sj_engine* eng, const sjb_schema* schema, const sjb_limits* base,
+                         const sjb_query* sample, int32_t n, int32_t reps, sjb_limits* chosen,
+                         sjb_tune_report* report);
+
 /* ------------------------------------------------------------- serving ---- */
 typedef struct sjs_server sjs_server;
 

@@ -1,7 +1,7 @@
 """Compile the reference's own SSB drivers into oracle/_ref/ -- TEST INFRASTRUCTURE.
 
-The driver sources are compiled where they lie under the reference tree
-(default /root/reference, override with CRYSTAL_OPT_REF); nothing is copied.
+The driver sources are compiled where they lie under the reference tree named
+by CRYSTAL_OPT_REF (nothing is built when it is unset); nothing is copied.
 Each binary is one driver -- src/ssb-jo/q33/<order>-<lip|naive>.cu wrapped by
 ref_runner.cu, or one of SHAPE_SOURCES (the other queries' drivers) wrapped by
 ref_runner_shapes.cu -- the wrapper supplying main() and the synthetic columns.  The reference's
@@ -20,7 +20,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF = os.environ.get("CRYSTAL_OPT_REF", "/root/reference")
+REF = os.environ.get("CRYSTAL_OPT_REF", "")
 ORDERS = range(6)
 METHODS = ("lip", "naive")
 
@@ -30,7 +30,7 @@ def binary(order: int, method: str) -> str:
 
 
 def available() -> bool:
-    return os.path.isdir(os.path.join(REF, "src", "ssb-jo", "q33"))
+    return bool(REF) and os.path.isdir(os.path.join(REF, "src", "ssb-jo", "q33"))
 
 
 def _compile(order: int, method: str) -> str:

@@ -12,6 +12,14 @@ for sub in ("crystal-opt_b200", "oracle"):
         sys.path.insert(0, p)
 
 
+if "CRYSTAL_OPT_REF" not in os.environ:  # the reference tree the build recipe uses, when present
+    sys.path.insert(0, ROOT)
+    from __graft_entry__ import REFERENCE_TREE  # noqa: E402
+
+    if os.path.isdir(REFERENCE_TREE):
+        os.environ["CRYSTAL_OPT_REF"] = REFERENCE_TREE
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
 

@@ -179,3 +179,24 @@ def test_cached_filter_regrouped(oracle, engine, star):
         assert b.stats().filters_cached > 0
     finally:
         b.close()
+
+
+def test_probe_shape_tuner(oracle, engine, star):
+    """sjb_batch_tune: every candidate probe shape (CTA size x shared-memory group
+    partials) gives the same groups, and a batch with the chosen shape matches
+    the oracle."""
+    sc, host, dev = star
+    rng = random.Random(6)
+    qs = [ss.random_query(rng, sc, len_range=(100_000, None)) for _ in range(24)]
+    shape, rep = ss.tune_batch(engine, sc, dev, qs, reps=2)
+    assert rep.mismatches == 0 and rep.candidates >= 6
+    assert shape["threads"] in (256, 512, 1024) and shape["smem_group_entries"] in (2048, 6144, 12288)
+    assert 0 < rep.best_probe_ms <= rep.default_probe_ms
+    b = ss.Batch(engine, sc, dev, **shape)
+    try:
+        got = b.run(qs)
+    finally:
+        b.close()
+    want = _oracle(oracle, sc, host, qs)
+    for i, (g, w) in enumerate(zip(got, want)):
+        assert g == w, i

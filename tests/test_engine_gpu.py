@@ -158,6 +158,11 @@ def test_prepared_query_rebuild_and_reprobe(sj, oracle, engine, small):
     assert st.groups == 24
     assert st.step_in[0] == SMALL.fact_rows
     assert st.error_flags == 0
+    for _ in range(3):  # probes over one build: the same groups and per-probe counters each time
+        pq.probe()
+        assert pq.fetch() == want
+        st = pq.stats()
+        assert st.rows_scanned == SMALL.fact_rows and st.groups == 24 and st.step_in[0] == SMALL.fact_rows
     pq.release()
 
 
