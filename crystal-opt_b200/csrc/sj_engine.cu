@@ -488,7 +488,8 @@ extern "C" sj_status sj_query_build(sj_query* q, void* stream) {
   if (!q) return fail(SJ_ERR_INVALID_ARGUMENT, "NULL query");
   cudaStream_t st = (cudaStream_t)stream;
   SJ_CUDA(cudaSetDevice(q->eng->device));
-  SJ_CUDA(cudaEventRecord(q->ev_start, st));
+  const bool events = q->plan.tune.record_events != 0;
+  if (events) SJ_CUDA(cudaEventRecord(q->ev_start, st));
   // the scan kernel clears the hash tables and filters, the compaction kernel
   // leaves the group sums zero; the whole region is cleared only after prepare
   // and after an error
@@ -508,7 +509,7 @@ extern "C" sj_status sj_query_build(sj_query* q, void* stream) {
   // the insert walks only the listed qualifying rows: a smaller grid
   const dim3 igrid(std::max(1u, std::min<uint32_t>(bx, (uint32_t)q->eng->sm_count * 2)), (unsigned)q->plan.n_dims);
   SJ_CUDA(launch_windowed(sj_dim_insert, igrid, dim3(256), 4 * max_pwords, st, L2Window{}, true, q->rt));
-  SJ_CUDA(cudaEventRecord(q->ev_built, st));
+  if (events) SJ_CUDA(cudaEventRecord(q->ev_built, st));
   q->built = true;
   q->probed_since_build = false;
   q->stream = st;
@@ -533,7 +534,7 @@ extern "C" sj_status sj_query_probe(sj_query* q, void* stream) {
   }
   SJ_CUDA(launch_finalize(q->rt, (uint32_t)q->group_capacity, st, true));
   q->groups_clean = true;
-  SJ_CUDA(cudaEventRecord(q->ev_probed, st));
+  if (q->plan.tune.record_events) SJ_CUDA(cudaEventRecord(q->ev_probed, st));
   q->probed = true;
   q->stream = st;
   return SJ_OK;
@@ -592,8 +593,10 @@ extern "C" sj_status sj_query_get_stats(sj_query* q, sj_query_stats* out) {
   out->reorders = desc.reorders;
   out->error_flags = desc.error_flags;
   float ms = 0.f;
-  if (q->built && cudaEventElapsedTime(&ms, q->ev_start, q->ev_built) == cudaSuccess) out->build_ms = ms;
-  if (q->probed && cudaEventElapsedTime(&ms, q->ev_built, q->ev_probed) == cudaSuccess) out->probe_ms = ms;
+  if (q->plan.tune.record_events) {
+    if (q->built && cudaEventElapsedTime(&ms, q->ev_start, q->ev_built) == cudaSuccess) out->build_ms = ms;
+    if (q->probed && cudaEventElapsedTime(&ms, q->ev_built, q->ev_probed) == cudaSuccess) out->probe_ms = ms;
+  }
   cudaGetLastError();
   return SJ_OK;
 }

@@ -65,7 +65,7 @@ class SjDim(C.Structure):
 class SjTuning(C.Structure):
     _fields_ = [("threads", C.c_int32), ("chunk_rows", C.c_int32), ("stages", C.c_int32),
                 ("ctas_per_sm", C.c_int32), ("compact_threshold", C.c_int32),
-                ("bf_smem_bytes", C.c_int32)]
+                ("bf_smem_bytes", C.c_int32), ("record_events", C.c_int32)]
 
 
 class SjPlan(C.Structure):

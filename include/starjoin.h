@@ -101,6 +101,9 @@ typedef struct sj_tuning {
   int32_t ctas_per_sm;        /* persistent CTAs per SM (1..4) */
   int32_t compact_threshold;  /* survivors queued before a compaction round (0 = threads) */
   int32_t bf_smem_bytes;      /* shared-memory budget for Bloom filters */
+  int32_t record_events;      /* 1: CUDA events around each build and probe, for the build_ms /
+                                 probe_ms of sj_query_get_stats (0: none; an event between the
+                                 build and the probe holds the probe's launch until the build ends) */
 } sj_tuning;
 
 typedef struct sj_plan {
@@ -146,7 +149,7 @@ typedef struct sj_query_stats {
   uint64_t groups;                     /* non-empty groups */
   uint64_t reorders;                   /* adaptive LIP re-rankings (all CTAs) */
   uint32_t error_flags;                /* device-side error bits (0 = none) */
-  float build_ms, probe_ms;            /* CUDA-event times of the last run */
+  float build_ms, probe_ms;            /* CUDA-event times of the last run (tune.record_events) */
   int32_t bf_blocked[SJ_MAX_DIMS];     /* 1: the dimension's filter was built blocked, 0: direct */
 } sj_query_stats;
 

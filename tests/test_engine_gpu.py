@@ -110,7 +110,8 @@ def test_row_ranges_and_ragged_tails(sj, oracle, engine, small, begin, end):
 
 @pytest.mark.parametrize("tune", [dict(threads=256), dict(threads=768), dict(stages=2), dict(stages=12, chunk_rows=4096),
                                   dict(chunk_rows=4096), dict(chunk_rows=16384, stages=3),
-                                  dict(bf_smem_bytes=0), dict(ctas_per_sm=2, stages=2, chunk_rows=4096)])
+                                  dict(bf_smem_bytes=0), dict(ctas_per_sm=2, stages=2, chunk_rows=4096),
+                                  dict(record_events=1)])
 def test_launch_geometry_does_not_change_results(sj, oracle, engine, small, tune):
     host, dev = small
     want = oracle.run(sj.q33_query(SMALL), host)
@@ -164,6 +165,29 @@ def test_prepared_query_rebuild_and_reprobe(sj, oracle, engine, small):
         st = pq.stats()
         assert st.rows_scanned == SMALL.fact_rows and st.groups == 24 and st.step_in[0] == SMALL.fact_rows
     pq.release()
+
+
+def test_rebuilds_follow_changed_dimension_rows(sj, oracle, engine, small, torch_cuda):
+    """Prepared re-builds over dimension columns changed in place: every build
+    clears the tables and filters the previous one set, so each round's groups
+    match the oracle on that round's columns."""
+    host, dev = small
+    cols = {k: v.clone() for k, v in dev.items()}
+    h = {k: v.copy() for k, v in host.items()}
+    q = sj.q33_query(SMALL, order=(0, 1, 2), adaptive=False)
+    pq = engine.prepare(q, cols, SMALL.fact_rows)
+    rng = np.random.default_rng(11)
+    try:
+        for r in range(6):
+            if r:  # new city attributes: a different set of customers and suppliers qualifies
+                for col in ("c_city", "s_city"):
+                    h[col] = rng.integers(0, 250, size=h[col].shape[0]).astype(np.int32)
+                    cols[col].copy_(torch_cuda.from_numpy(h[col]))
+            pq.build()
+            pq.probe()
+            assert pq.fetch() == oracle.run(q, h), r
+    finally:
+        pq.release()
 
 
 def test_invalid_arguments_are_reported(sj, engine, small):
