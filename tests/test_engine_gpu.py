@@ -283,13 +283,14 @@ def test_q33_full_size(sj, engine, full, full_want, order):
 
 
 def _probe_ms(engine, q, cols, rows, reps=5):
-    pq = engine.prepare(q, cols, rows)
+    pq = engine.prepare(q, cols, rows, tune={"record_events": 1})  # build_ms / probe_ms in the stats
     times = []
     for _ in range(reps):
         pq.build()
         pq.probe()
         pq.fetch()
         times.append(pq.stats().probe_ms)
+    assert min(times) > 0
     st = pq.stats()
     res = pq.fetch()
     pq.release()
