@@ -367,6 +367,20 @@ cudaError_t sjb_launch_zero_groups(const SjbStep* step, uint64_t zero_mask, SjbA
 // Lane j of a warp owns slot 32*w + j.  Lanes first load the bitmap word w of
 // query slots j and j + 32 in parallel; each query's word then reaches every
 // lane by shuffle, and its bit j lands in bit q of lane j's mask word.
+// 32 x 32 bit transpose across a warp: lane l holds row l (bit c = element
+// [l][c]) and returns column l (bit q = element [q][l]).  Five butterfly stages;
+// stage j swaps the off-diagonal j x j blocks between lanes l and l ^ j, the
+// shuffle-network form of the recursive block transpose (Warren, Hacker's
+// Delight, 7-3).
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, uint32_t lane) {
+#pragma unroll
+  for (uint32_t j = 16, m = 0x0000FFFFu; j; j >>= 1, m ^= m << j) {
+    const uint32_t y = __shfl_xor_sync(kFull, x, j);
+    x = (lane & j) ? ((x & ~m) | ((y & ~m) >> j)) : ((x & m) | ((y & m) << j));
+  }
+  return x;
+}
+
 __global__ void __launch_bounds__(256) sjb_compose_kernel(const __grid_constant__ SjbSchemaRt S,
                                                           const SjbStep* __restrict__ G) {
   const uint32_t d = blockIdx.y;
@@ -379,14 +393,8 @@ __global__ void __launch_bounds__(256) sjb_compose_kernel(const __grid_constant_
   const uint32_t* bm_lo = ((use >> lane) & 1ull) ? G->bm[lane][d] : nullptr;
   const uint32_t* bm_hi = ((use >> (lane + 32)) & 1ull) ? G->bm[lane + 32][d] : nullptr;
   for (uint32_t w = blockIdx.x * (blockDim.x / 32u) + (threadIdx.x >> 5); w < words; w += warps) {
-    const uint32_t lo = bm_lo ? __ldg(bm_lo + w) : 0u;
-    const uint32_t hi = bm_hi ? __ldg(bm_hi + w) : 0u;
-    uint32_t m_lo = 0, m_hi = 0;
-#pragma unroll 8
-    for (int q = 0; q < 32; ++q) {
-      m_lo |= ((__shfl_sync(kFull, lo, q) >> lane) & 1u) << q;
-      m_hi |= ((__shfl_sync(kFull, hi, q) >> lane) & 1u) << q;
-    }
+    const uint32_t m_lo = warp_transpose32(bm_lo ? __ldg(bm_lo + w) : 0u, lane);
+    const uint32_t m_hi = warp_transpose32(bm_hi ? __ldg(bm_hi + w) : 0u, lane);
     const uint32_t s = w * 32u + lane;
     if (s < R.len) R.mask[s] = (uint64_t)m_lo | ((uint64_t)m_hi << 32);
   }
