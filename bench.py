@@ -32,7 +32,7 @@ FACT_ROWS = 120_000_000
 CUST_ROWS, SUPP_ROWS = 600_000, 40_000
 SEED = 0x5EED0002
 BYTES_PER_ROW = 16  # 3 FK columns + revenue, int32 (algorithmic bytes per fact row)
-PROBE_EVERY = 8  # timed steps per probe-event sample
+PROBE_EVERY = 20  # timed steps per probe-event sample
 METRIC = "fact rows/s, 3-dim LIP star join (SSB Q3.3 shape)"
 
 
@@ -314,8 +314,8 @@ def run_engine(args):
     result = pq.fetch(stream=sptr)
 
     # the probe's own duration: CUDA events around it on every PROBE_EVERY-th timed
-    # step (an event pair between the build and the probe costs about 7 us of a
-    # 0.2 ms step, so sampling keeps the instrumentation out of ms_per_step)
+    # step (an event between the build and the probe holds the probe's launch until
+    # the build drains, so sampling keeps that instrumentation out of ms_per_step)
     probe_every = PROBE_EVERY if args.steps >= 4 * PROBE_EVERY else 1
     probe_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                 for _ in range(0, args.steps, probe_every)]

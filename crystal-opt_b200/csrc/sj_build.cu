@@ -62,7 +62,11 @@ __global__ void __launch_bounds__(256) sj_dim_insert(const __grid_constant__ SjP
       write_dict(D, prefix, pwords);
       if (threadIdx.x == 0) desc->dim[d].n_codes = s_total;
     }
-    if (d == 0 && threadIdx.x < 32) {  // the query-wide fields, by warp 0
+  }
+  // the query-wide fields, by warp 0 of dimension 0's last block: the blocks at
+  // the front of the grid take the listed rows, so this overlaps the inserts
+  if (blockIdx.x == gridDim.x - 1) {
+    if (d == 0 && threadIdx.x < 32) {
       const uint32_t lane = threadIdx.x;
       uint32_t n_codes[kMaxDims] = {0, 0, 0, 0}, stride[kMaxDims], ins[kMaxDims] = {0, 0, 0, 0};
 #pragma unroll

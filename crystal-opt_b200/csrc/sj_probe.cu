@@ -665,7 +665,22 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
           aborted = true;
           break;
         }
-        // adaptive re-ranking of the filter order for the chunks issued from here on
+        const uint32_t chunk = blockIdx.x + it * gridDim.x;
+        const uint32_t d = c.order[issue_ver][0];
+        c.stage_ver[s] = issue_ver;
+        const uint64_t start = base_row + (uint64_t)chunk * CH;
+        const uint64_t rows = min((uint64_t)CH, P.row_end - start);
+        const uint32_t bytes = (uint32_t)(rows & ~3ull) * 4u;
+        fence_proxy_async_smem();
+        if (bytes) {
+          mbar_arrive_expect_tx(&full[s], bytes);
+          bulk_g2s(stage + (size_t)s * CH, P.dim[d].fact_fk + start, bytes, &full[s], pol_first);
+        } else {
+          mbar_arrive(&full[s]);
+        }
+        // adaptive re-ranking of the filter order for the chunks issued after this one:
+        // evaluated once this chunk's copy is in flight, so the evaluation overlaps
+        // the wait for the next free stage instead of delaying a copy
         if (P.lip && P.adaptive && P.n_dims > 1 && it >= last_switch + 2 * S &&
             (it == 2 * S || it % G.reorder_period == 0)) {
           float rate[kMaxDims];
@@ -695,19 +710,6 @@ __global__ void __launch_bounds__((NWC + 1) * 32, 1) sj_probe_kernel(const __gri
             last_switch = it;
             c.reorders++;
           }
-        }
-        const uint32_t chunk = blockIdx.x + it * gridDim.x;
-        const uint32_t d = c.order[issue_ver][0];
-        c.stage_ver[s] = issue_ver;
-        const uint64_t start = base_row + (uint64_t)chunk * CH;
-        const uint64_t rows = min((uint64_t)CH, P.row_end - start);
-        const uint32_t bytes = (uint32_t)(rows & ~3ull) * 4u;
-        fence_proxy_async_smem();
-        if (bytes) {
-          mbar_arrive_expect_tx(&full[s], bytes);
-          bulk_g2s(stage + (size_t)s * CH, P.dim[d].fact_fk + start, bytes, &full[s], pol_first);
-        } else {
-          mbar_arrive(&full[s]);
         }
       }
       if (aborted) {
