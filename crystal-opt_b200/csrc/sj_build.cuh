@@ -119,23 +119,19 @@ __device__ __forceinline__ T sel4(const T (&a)[kMaxDims], uint32_t i) {
   return i == 0 ? a[0] : i == 1 ? a[1] : i == 2 ? a[2] : a[3];
 }
 
-// Permutation number p (0 <= p < n!) of 0..n-1 in lexicographic order, by the
-// factorial number system; entries from n on are left as their index.
+// Permutation number p (0 <= p < n!) of 0..n-1 in lexicographic order; entries
+// from n on are their index.  The permutations are packed one byte each (entry
+// i in bits 2i..2i+1), eight to a 64-bit word, so lane p reads its own with two
+// shifts instead of factorial-base divisions.
 __device__ __forceinline__ void nth_perm(uint32_t p, uint32_t n, uint32_t (&perm)[kMaxDims]) {
-  uint32_t avail = (1u << n) - 1u;
-  uint32_t fact = n == 4 ? 6u : n == 3 ? 2u : 1u;  // (n-1)!
+  uint64_t w;
+  if (n == 4) w = p < 8 ? 0xb1e16c9c78d8b4e4ull : (p < 16 ? 0x36c672d22d8d39c9ull : 0x1b4b278763931e4eull);
+  else if (n == 3) w = 0xc6d2c9e1d8e4ull;
+  else if (n == 2) w = 0xe1e4ull;
+  else w = 0xe4ull;  // identity
+  const uint32_t code = (uint32_t)(w >> (8u * (p & 7u))) & 0xFFu;
 #pragma unroll
-  for (uint32_t i = 0; i < kMaxDims; ++i) {
-    perm[i] = i;
-    if (i >= n) continue;
-    const uint32_t q = p / fact;
-    p -= q * fact;
-    uint32_t a = avail;
-    for (uint32_t k = 0; k < q; ++k) a &= a - 1u;  // the q-th unused dimension
-    perm[i] = (uint32_t)__ffs(a) - 1u;
-    avail &= ~(1u << perm[i]);
-    if (n - 1u - i > 1u) fact /= n - 1u - i;
-  }
+  for (uint32_t i = 0; i < kMaxDims; ++i) perm[i] = (code >> (2u * i)) & 3u;
 }
 
 // Starting LIP order and filter placement for the probe, by one warp (`lane`).
