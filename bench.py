@@ -374,7 +374,7 @@ def run_engine(args):
                                  "bandwidth" if traffic else
                                  "probe kernel: no DRAM capture for this setting, so achieved uses the 16 B/row "
                                  "algorithmic model"},
-            "gpu_launches": 4 * args.steps,  # scan, insert, probe, compaction
+            "gpu_launches": 5 * args.steps,  # head clear, scan, insert, probe, compaction
             "groups": len(result), "groups_merged_ok": groups_ok,
             "stats": {"step_in": list(stats.step_in)[:6], "step_out": list(stats.step_out)[:6],
                       "bf_inserted": list(stats.bf_inserted)[:3], "bf_words": list(stats.bf_words)[:3],

@@ -18,6 +18,15 @@
 
 namespace sj {
 
+// Clears the descriptor and payload bitmaps a build starts from (16-byte
+// multiple); the scan kernel, launched as its programmatic dependent, clears the
+// hash tables meanwhile and waits for this grid before its first write there.
+__global__ void __launch_bounds__(256) sj_clear_head(uint4* __restrict__ head, uint64_t n16) {
+  pdl_launch_dependents();
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += (uint64_t)gridDim.x * blockDim.x)
+    head[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 __global__ void __launch_bounds__(256) sj_dim_scan(const __grid_constant__ SjPlanRt P) {
   pdl_launch_dependents();  // sj_dim_insert may be scheduled; it waits for this grid
   // clear the hash tables and filters sj_dim_insert fills (every block of the grid)
@@ -28,6 +37,7 @@ __global__ void __launch_bounds__(256) sj_dim_scan(const __grid_constant__ SjPla
     for (uint64_t i = ((uint64_t)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += nt)
       z[i] = make_uint4(0u, 0u, 0u, 0u);
   }
+  pdl_wait();  // launched after sj_clear_head: the descriptor and payload bitmaps are clear
   const uint32_t d = blockIdx.y;
   if (d >= P.n_dims) return;
   SjDesc* desc = P.desc;

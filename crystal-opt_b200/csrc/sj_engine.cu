@@ -27,6 +27,7 @@ cudaError_t launch_probe(const SjPlanRt& P, const SjProbeGeom& G, uint32_t rows_
                          const L2Window& w, bool pdl);
 cudaError_t launch_finalize(const SjPlanRt& P, uint32_t group_capacity, cudaStream_t st, bool pdl);
 __global__ void sj_dim_scan(const __grid_constant__ SjPlanRt P);
+__global__ void sj_clear_head(uint4* __restrict__ head, uint64_t n16);
 __global__ void sj_dim_insert(const __grid_constant__ SjPlanRt P);
 }  // namespace sj
 
@@ -493,7 +494,15 @@ extern "C" sj_status sj_query_build(sj_query* q, void* stream) {
   // the scan kernel clears the hash tables and filters, the compaction kernel
   // leaves the group sums zero; the whole region is cleared only after prepare
   // and after an error
-  SJ_CUDA(cudaMemsetAsync(q->arena, 0, q->groups_clean ? q->head_bytes : q->zero_bytes, st));
+  const bool head_only = q->groups_clean;
+  if (head_only) {  // a kernel, so the scan can be its programmatic dependent
+    const uint64_t n16 = q->head_bytes / 16;
+    const uint32_t blocks = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((n16 + 255) / 256, 64));
+    sj_clear_head<<<blocks, 256, 0, st>>>(reinterpret_cast<uint4*>(q->arena), n16);
+    SJ_CUDA(cudaGetLastError());
+  } else {
+    SJ_CUDA(cudaMemsetAsync(q->arena, 0, q->zero_bytes, st));
+  }
   q->groups_clean = true;
   int64_t max_rows = 1;
   uint32_t max_pwords = 1;
@@ -504,8 +513,7 @@ extern "C" sj_status sj_query_build(sj_query* q, void* stream) {
   uint32_t bx = (uint32_t)std::min<int64_t>((max_rows + 255) / 256, (int64_t)q->eng->sm_count * 8);
   if (bx < 1) bx = 1;
   dim3 grid(bx, (unsigned)q->plan.n_dims);
-  sj_dim_scan<<<grid, 256, 0, st>>>(q->rt);
-  SJ_CUDA(cudaGetLastError());
+  SJ_CUDA(launch_windowed(sj_dim_scan, grid, dim3(256), 0, st, L2Window{}, head_only, q->rt));
   // the insert walks only the listed qualifying rows: a smaller grid
   const dim3 igrid(std::max(1u, std::min<uint32_t>(bx, (uint32_t)q->eng->sm_count * 2)), (unsigned)q->plan.n_dims);
   SJ_CUDA(launch_windowed(sj_dim_insert, igrid, dim3(256), 4 * max_pwords, st, L2Window{}, true, q->rt));
