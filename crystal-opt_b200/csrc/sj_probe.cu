@@ -841,19 +841,23 @@ __global__ void __launch_bounds__(256) sj_finalize_kernel(const __grid_constant_
   pdl_wait();  // the probe's group sums are complete
   SjDesc* desc = P.desc;
   const uint32_t n_groups = desc->n_groups;
+  uint32_t n_codes[kMaxDims], stride[kMaxDims];  // read once, beside n_groups
+#pragma unroll
+  for (uint32_t d = 0; d < kMaxDims; ++d) {
+    const bool grouped = d < P.n_dims && P.dim[d].grouped;
+    n_codes[d] = grouped && desc->dim[d].n_codes ? desc->dim[d].n_codes : 1u;
+    stride[d] = grouped ? desc->dim[d].group_stride : 1u;
+  }
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < n_groups; g += gridDim.x * blockDim.x) {
     const unsigned long long cnt = P.g_cnt[g];
     if (!cnt) continue;
     const uint32_t pos = atomicAdd(&desc->groups_out, 1u);
     if (pos >= P.group_capacity) continue;  // cannot happen: at most n_groups rows
     sj_group_row r;
+#pragma unroll
     for (uint32_t d = 0; d < kMaxDims; ++d) {
       r.attr[d] = 0;
-      if (d < P.n_dims && P.dim[d].grouped) {
-        const uint32_t n = desc->dim[d].n_codes ? desc->dim[d].n_codes : 1u;
-        const uint32_t code = (g / desc->dim[d].group_stride) % n;
-        r.attr[d] = P.dim[d].dict[code];
-      }
+      if (d < P.n_dims && P.dim[d].grouped) r.attr[d] = P.dim[d].dict[(g / stride[d]) % n_codes[d]];
     }
     r.count = cnt;
     r.sum = P.g_sum[g];
